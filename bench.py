@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""mDPD particle-steps/s on B200: batched (256 uneven boxes) vs plain single-box, with the
+pair-kernel HBM roofline on a 4M-particle box, served p50/p99 latency, the CPU baseline and
+the end-to-end number through the C ABI.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one rank per GPU, each rank stepping its own 256-box set (weak
+scaling, no collective on the data path); rank 0 prints ONE JSON line.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "usermeso-2.0-mdpd_b200"))
+
+RHO = 6.05
+RC, SKIN = 1.0, 0.3
+NBAR = RHO * 4.0 / 3.0 * math.pi * (RC + SKIN) ** 3          # list entries per particle, 55.7
+B_RHO = 24 + 4 * NBAR                                         # density pass bytes / particle
+B_F = 52 + 4 * NBAR                                           # force pass bytes / particle
+WORKLOAD = ("batched mDPD: 256 periodic boxes, N log-uniform in [2k,200k], rho 6.05, "
+            "A~U[-50,-30], B~U[20,30], r_d~U[0.7,0.8], kT 1, gamma 4.5, dt 0.01, skin 0.3")
+
+
+def config4(seed, nbox=256):
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(np.log(2000), np.log(200000), nbox)).astype(int)
+    A = rng.uniform(-50, -30, nbox); B = rng.uniform(20, 30, nbox); rd = rng.uniform(0.7, 0.8, nbox)
+    return [dict(n=int(n[k]), L=(n[k] / RHO) ** (1 / 3), A=float(A[k]), B=float(B[k]), rd=float(rd[k]),
+                 seed=int(1000 + k + 100000 * seed), init_seed=int(7 + k + 100000 * seed)) for k in range(nbox)]
+
+
+def specs_of(cfg):
+    import mdpd
+    return [mdpd.box_spec(c["n"], c["L"], A=c["A"], B=c["B"], cut_r=c["rd"], seed=c["seed"],
+                          init_seed=c["init_seed"]) for c in cfg]
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, dev):
+        self.dev, self.lines, self.p = dev, [], None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.p = None
+        return self
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0])); mx = float(f[1])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[3 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    """DRAM bytes per launch of the force/density passes from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "pair_passes_4M_ncu.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_baseline(cfg, budget_s=15.0, threads=0):
+    """The oracle's FP64 engine (OpenMP over all host threads) on a bounded sample of boxes."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    ncores = threads or os.cpu_count() or 1
+    order = sorted(range(len(cfg)), key=lambda k: cfg[k]["n"])
+    pick = [order[len(order) // 2], order[len(order) // 4], order[(3 * len(order)) // 4]]
+    done_ps, spent = 0.0, 0.0
+    sample = []
+    for k in pick:
+        c = cfg[k]
+        rng = np.random.default_rng(c["init_seed"])
+        x = rng.uniform(0, c["L"], (c["n"], 3)); v = rng.normal(0, 1, (c["n"], 3)); v -= v.mean(0)
+        sim = oracle.Sim(x, v, (0, 0, 0), (c["L"],) * 3, A=c["A"], B=c["B"], cut_r=c["rd"], seed=c["seed"],
+                         nthreads=ncores)
+        sim.setup()
+        sim.run(1)
+        t0 = time.perf_counter()
+        sim.run(2)
+        dt = (time.perf_counter() - t0) / 2
+        steps = max(1, min(200, int((budget_s / len(pick)) / max(dt, 1e-6))))
+        t0 = time.perf_counter()
+        sim.run(steps)
+        el = time.perf_counter() - t0
+        sim.close()
+        done_ps += c["n"] * steps
+        spent += el
+        sample.append(f"box n={c['n']} x {steps} steps")
+    return {"value": done_ps / spent, "unit": "particle-steps/s", "cores": ncores, "kind": "port",
+            "sample": "oracle FP64 engine (OpenMP) on 3 boxes of the 256-box set: " + "; ".join(sample)}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU path (the oracle port; the 2013 reference has no
+    CPU mDPD style) on the host cores, same workload, bounded sample per step."""
+    if rank != 0:
+        return
+    cfg = config4(seed=1)
+    base = cpu_baseline(cfg, budget_s=max(5.0, 0.3 * (args.steps + args.warmup)))
+    line = {"impl": "reference", "metric": "mDPD particle-steps/s (batched 256-box workload)",
+            "value": base["value"], "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded)", "config": {"workload": WORKLOAD},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours")
+    ap.add_argument("--no-extras", action="store_true", help="skip plain/served/roofline/cpu legs")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0")); world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    import mdpd
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    # ---- headline: batched 256-box workload, resident in HBM -------------------------------
+    cfg = config4(seed=1 + rank)
+    specs = specs_of(cfg)
+    ntot = sum(c["n"] for c in cfg)
+    b = mdpd.Batch(specs, device=local)
+    b.setup()
+    b.step(args.warmup)
+    r0 = b.rebuild_steps()
+    barrier()
+    with Clocks(local) as clk:
+        barrier()
+        ms = b.time(args.steps)              # CUDA events on the batch stream, K steps
+        barrier()
+    r1 = b.rebuild_steps()
+    t_max = max_over_ranks(ms * args.steps / 1e3)
+    value = sum_over_ranks(ntot * args.steps) / t_max
+    gpu_launches = 3 * args.steps + 17 * (r1 - r0)
+    b.close()
+
+    line = {"metric": "mDPD particle-steps/s (batched 256-box workload)", "value": value,
+            "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 pair / f64 integrate", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "boxes": 256, "particles_per_gpu": ntot,
+                       "l2": "inputs larger than L2: state + lists of ~%d particles (%.1f GB)" % (
+                           ntot, ntot * 1.1e-6),
+                       "parallelism": f"replicas x{world} (independent box sets)"},
+            "clocks": clk.summary(), "gpu_launches": gpu_launches}
+
+    if not args.no_extras and rank == 0:
+        # ---- e2e through the C ABI: host arrays in, K steps, host arrays out ----------------
+        rng = np.random.default_rng(11)
+        xs, vs = [], []
+        for c in cfg:
+            xs.append(rng.uniform(0, c["L"], (c["n"], 3)))
+            v = rng.normal(0, 1, (c["n"], 3)); vs.append(v - v.mean(0))
+        t0 = time.perf_counter()
+        sp = [mdpd.box_spec(c["n"], c["L"], A=c["A"], B=c["B"], cut_r=c["rd"], seed=c["seed"], x=x, v=v)
+              for c, x, v in zip(cfg, xs, vs)]
+        be = mdpd.Batch(sp, device=local)
+        be.setup()
+        be.step(args.steps)
+        temps = [be.thermo(k).temp for k in range(0, 256, 64)]
+        outs = [be.state(k) for k in range(256)]
+        e2e_s = time.perf_counter() - t0
+        be.close()
+        line["e2e"] = {"value": ntot * args.steps / e2e_s, "unit": "particle-steps/s",
+                       "h2d_bytes_per_step": int(48 * ntot / args.steps),
+                       "d2h_bytes_per_step": int(48 * ntot / args.steps),
+                       "note": "create+upload of all 256 boxes, setup, K steps, thermo and full state download, "
+                               "wall clock"}
+        del outs, temps
+
+        # ---- plain single-box path on the same boxes (one box per launch sequence) ----------
+        plain_ps, plain_s = 0.0, 0.0
+        for s, c in zip(specs_of(cfg), cfg):
+            bb = mdpd.Batch([s], device=local)
+            bb.setup()
+            bb.step(3)
+            msb = bb.time(20)
+            plain_ps += c["n"] * 20
+            plain_s += msb * 20 / 1e3
+            bb.close()
+        line["plain"] = {"value": plain_ps / plain_s, "unit": "particle-steps/s",
+                         "note": "same 256 boxes, each stepped alone (20 steps, CUDA events)",
+                         "batched_over_plain": value / world / (plain_ps / plain_s)}
+
+        # ---- roofline: pair passes of the 4M-particle cubic box -----------------------------
+        n4 = 4_000_000
+        s4 = mdpd.box_spec(n4, (n4 / RHO) ** (1 / 3), A=-40.0, B=25.0, seed=4242, init_seed=99)
+        b4 = mdpd.Batch([s4], device=local)
+        b4.setup()
+        b4.step(args.warmup)
+        prof = b4.profile(max(10, args.steps // 2))
+        ms4 = b4.time(max(10, args.steps // 2))
+        b4.close()
+        peak, how = peaks()
+        t_pair = (prof["density_ms"] + prof["force_ms"]) / 1e3
+        achieved = (B_RHO + B_F) * n4 / t_pair / 1e9
+        tr = traffic_per_launch()
+        line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "peak_source": how,
+                            "traffic": tr.get("pair_bytes_per_step") if tr else None,
+                            "kernel": "pair passes (density + force), 4M-particle box",
+                            "bytes_per_particle": B_RHO + B_F, "nbar": NBAR,
+                            "density_ms": prof["density_ms"], "force_ms": prof["force_ms"],
+                            "density_frac": B_RHO * n4 / (prof["density_ms"] / 1e3) / 1e9 / peak,
+                            "force_frac": B_F * n4 / (prof["force_ms"] / 1e3) / 1e9 / peak,
+                            "integrate_ms": prof["integrate_ms"], "rebuild_ms_avg": prof["rebuild_ms"]}
+        line["single_box_4M"] = {"value": n4 / (ms4 / 1e3), "unit": "particle-steps/s", "ms_per_step": ms4}
+
+        # ---- served: Poisson arrivals of droplet/slab jobs (bounded sample of config 5) ------
+        srv = mdpd.Server(budget_bytes=int(150e9), device=local)
+        rng = np.random.default_rng(5)
+        njobs = 24
+        t_arr = np.cumsum(rng.exponential(1 / 20.0, njobs))
+        t0 = time.perf_counter()
+        ids = []
+        for k in range(njobs):
+            while time.perf_counter() - t0 < t_arr[k]:
+                time.sleep(0.001)
+            n = int(np.exp(rng.uniform(np.log(5000), np.log(2_000_000))))
+            steps = int(rng.integers(2000, 20001)) // 40
+            L = (2 * n / RHO) ** (1 / 3)
+            slab = rng.random() < 0.5
+            lo_f, hi_f = (0, 0, 0), (0, 0, 0)
+            sp = mdpd.box_spec(n, L, A=float(rng.uniform(-50, -30)), B=float(rng.uniform(20, 30)),
+                               cut_r=float(rng.uniform(0.7, 0.8)), seed=5000 + k, init_seed=900 + k,
+                               fill_lo=(0.25 * L, 0, 0) if slab else (0.103 * L,) * 3,
+                               fill_hi=(0.75 * L, L, L) if slab else (0.897 * L,) * 3)
+            ids.append(srv.submit(sp, steps))
+        srv.drain(timeout_s=600)
+        st = srv.stats()
+        srv.stop()
+        line["served"] = {"throughput": st["particle_steps_per_s"], "unit": "particle-steps/s",
+                          "step_ms_p50": st["step_ms_p50"], "step_ms_p99": st["step_ms_p99"],
+                          "job_s_p50": st["job_s_p50"], "job_s_p99": st["job_s_p99"], "jobs": int(st["jobs_done"]),
+                          "sample": f"{njobs} Poisson(20/s) droplet/slab jobs, N log-uniform 5k-2M, "
+                                    "steps U{2000..20000}/40, 150 GB budget"}
+
+        # ---- CPU baseline (oracle port on host cores) ---------------------------------------
+        line["cpu_baseline"] = cpu_baseline(cfg)
+
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,175 @@
+/*
+ * mdpd.h -- C ABI of the B200 DPD/mDPD timestep library (libmdpd.so).
+ *
+ * Drop-in boundary for the USER-MESO hot path.  In the reference, LAMMPS core reaches
+ * the path through its compile-time style registry and virtual methods:
+ *   PairStyle(mdpd/meso, MesoPairMDPD)        src/USER-MESO/pair_mdpd_meso.h:3
+ *   PairStyle(dpd/meso, MesoPairDPD)          src/USER-MESO/pair_dpd_meso.h:3
+ *   AtomStyle(mdpd/atomic/meso, ...)          src/USER-MESO/atom_vec_mdpd_atomic_meso.h:3
+ *   FixStyle(nve/meso / aboundary/rho/meso / addforce/meso / density/meso, ...)
+ *   IntegrateStyle(mvv/meso, ModifiedVerlet)  src/USER-MESO/mvv_meso.h:3-4
+ *   Input::file/one -> Force::create_pair / Modify::add_fix / Run::command (src/run.cpp:170-178)
+ * A caller replaces that chain by these entry points.  Every call returns an MDPD_* status;
+ * the library never exits the process (the reference aborts through error->all or
+ * raise(SIGABRT), src/USER-MESO/util_meso.h:100-101, and exits on OOM, engine_meso.h:126-145).
+ * All pointers are host pointers; the library owns every device allocation.
+ */
+#ifndef MDPD_H
+#define MDPD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDPD_OK 0
+#define MDPD_ERR_PARSE 1     /* malformed or unsupported script command            */
+#define MDPD_ERR_OOM 2       /* device allocation failed                            */
+#define MDPD_ERR_OVERFLOW 3  /* neighbour list / ghost / bin capacity exceeded      */
+#define MDPD_ERR_NAN 4       /* non-finite force                                    */
+#define MDPD_ERR_TIMEOUT 5   /* bounded device wait expired                         */
+#define MDPD_ERR_CUDA 6      /* CUDA runtime error                                  */
+#define MDPD_ERR_ARG 7       /* invalid argument                                    */
+#define MDPD_ERR_STATE 8     /* call out of order (e.g. run before the box exists)  */
+#define MDPD_ERR_BUDGET 9    /* serving: job does not fit the HBM budget            */
+
+typedef struct mdpd_s mdpd_t;
+
+typedef struct mdpd_opts {
+    int device;   /* CUDA device ordinal */
+    int verbose;  /* echo the thermo log to stdout */
+} mdpd_opts;
+
+typedef struct mdpd_thermo_t {
+    int64_t step;
+    int64_t natoms;
+    int64_t nbuild;       /* neighbour-list builds so far */
+    double temp;          /* compute temp/meso over all atoms, dof = 3N-3 */
+    double press;         /* compute pressure/meso scalar */
+    double pe;            /* total pair energy (E_pair * N) */
+    double ke;            /* 0.5 * sum m v^2 */
+    double virial[6];     /* xx yy zz xy xz yz, sums of the per-atom halved virials */
+    double momentum[3];
+    double temp_group;    /* temperature of the nve/meso group */
+    int32_t status;       /* device error bits */
+    int32_t pad;
+} mdpd_thermo_t;
+
+/* --- single box driven by the LAMMPS script surface ------------------------------------ */
+/* Input::one / Input::file (src/input.cpp) for the supported command subset */
+int mdpd_create(mdpd_t **h, const mdpd_opts *opts);
+int mdpd_command(mdpd_t *h, const char *line);
+int mdpd_file(mdpd_t *h, const char *path);
+/* Run::command + ModifiedVerlet::setup/run (src/run.cpp:170-178, mvv_meso.cu:203-572) */
+int mdpd_run(mdpd_t *h, int64_t nsteps);
+/* ModifiedVerlet::setup only: rebuild, density pass, force pass (mvv_meso.cu:203-283) */
+int mdpd_setup(mdpd_t *h);
+/* steps without setup, thermo or output (the inner loop of ModifiedVerlet::run) */
+int mdpd_step(mdpd_t *h, int64_t nsteps);
+int mdpd_natoms(mdpd_t *h, int64_t *n);
+/* state in tag order (row t-1 holds tag t): x,v 3*n doubles, tag/type n ints; NULL skips */
+int mdpd_get_state(mdpd_t *h, double *x, double *v, int32_t *tag, int32_t *type, int64_t n);
+/* replace positions/velocities (tag order); the next run/setup rebuilds */
+int mdpd_set_state(mdpd_t *h, const double *x, const double *v, int64_t n);
+/* compute temp/meso, pressure/meso, pe/meso (compute_temp_meso.cu:58-101,
+ * compute_pressure_meso.cu:98-150, compute_pe_meso.cu:66) */
+int mdpd_thermo(mdpd_t *h, mdpd_thermo_t *out);
+/* thermo log accumulated so far (LAMMPS thermo lines) */
+const char *mdpd_log(mdpd_t *h);
+const char *mdpd_last_error(mdpd_t *h);
+void mdpd_destroy(mdpd_t *h);
+
+/* --- internal arrays for parity checks (internal particle order) ------------------------
+ * name: "pos4" (float4, locals+ghosts), "vel4" (float4, locals+ghosts), "rho" (float,
+ * locals+ghosts), "force" (float4, locals), "count" (int, locals), "tag" (int, locals),
+ * "ghost_src" (int), "ghost_img" (int), "x" (double 3*n, locals, internal order),
+ * "list" (int, n_col*ceil32(n): the locally transposed table, neigh_list_meso.cu:143-147).
+ * sizes: returns the element count of a field in *count.                                 */
+int mdpd_field_size(mdpd_t *h, const char *name, int64_t *count);
+int mdpd_get_field(mdpd_t *h, const char *name, void *out, int64_t nbytes);
+/* box geometry: lo[3], hi[3], cen[3], mbin[3] as doubles, cutneighmax, n_col, nghost,
+ * n_bulk, nbuild (15 doubles) */
+int mdpd_geometry(mdpd_t *h, double *out15);
+/* neighbour pairs of the last build as (tag_i, tag_j), i local; *npairs on return */
+int mdpd_get_pairs(mdpd_t *h, int32_t *tag_i, int32_t *tag_j, int64_t cap, int64_t *npairs);
+
+/* --- pairwise RNG on explicit signature pairs (math_meso.h:465-473) --------------------- */
+int mdpd_gaussian(const uint32_t *si, const uint32_t *sj, double *exact, float *fast, int64_t n);
+
+/* --- batched boxes: many independent boxes stepped by one graph per step ---------------- */
+typedef struct mdpd_batch_s mdpd_batch_t;
+
+typedef struct mdpd_box_spec {
+    int32_t style;        /* 0 mdpd/meso, 1 dpd/meso */
+    int32_t n;            /* particles */
+    double lo[3], hi[3];
+    double A, B, gamma, kT, cut, cut_r, cut_rho;  /* mdpd; dpd uses A (a0), gamma, cut, sigma */
+    double sigma;         /* dpd only */
+    double dt, skin, rho_est, mass;
+    uint32_t seed;        /* pair RNG seed */
+    int32_t every, delay, check;
+    int32_t exact_rng;
+    /* initial state (tag order, tags 1..n); when x is NULL the box is filled uniformly
+     * at random from init_seed and v drawn from a Maxwell distribution at kT with zero
+     * net momentum */
+    const double *x, *v;
+    uint64_t init_seed;
+    double fill_lo[3], fill_hi[3];  /* random fill region (fill_hi <= fill_lo: whole box) */
+} mdpd_box_spec;
+
+int mdpd_batch_create(mdpd_batch_t **b, const mdpd_box_spec *specs, int32_t nbox, const mdpd_opts *opts);
+int mdpd_batch_setup(mdpd_batch_t *b);
+int mdpd_batch_step(mdpd_batch_t *b, int64_t nsteps);
+int mdpd_batch_thermo(mdpd_batch_t *b, int32_t box, mdpd_thermo_t *out);
+int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int64_t n);
+/* tune threads-per-particle of the pair passes by timing (project autotuner) */
+int mdpd_batch_tune(mdpd_batch_t *b, int32_t *tpp_density, int32_t *tpp_force);
+/* last per-step device time in milliseconds measured with CUDA events over nsteps */
+int mdpd_batch_time(mdpd_batch_t *b, int64_t nsteps, double *ms_per_step);
+/* nsteps un-captured steps with CUDA events around each kernel group (same kernels as the
+ * graph): per-step ms of [integrate, rebuild, density, force] and the number of steps whose
+ * rebuild ran (5 doubles) */
+int mdpd_batch_profile(mdpd_batch_t *b, int64_t nsteps, double *out5);
+/* steps whose rebuild body ran since creation (device counter) */
+int mdpd_batch_rebuild_steps(mdpd_batch_t *b, int64_t *n);
+const char *mdpd_batch_last_error(mdpd_batch_t *b);
+void mdpd_batch_destroy(mdpd_batch_t *b);
+
+/* --- serving: admission by HBM budget, resident state, continuous batching -------------- */
+typedef struct mdpd_server_s mdpd_server_t;
+
+typedef struct mdpd_job_spec {
+    mdpd_box_spec box;
+    int64_t nsteps;
+    int32_t keep_state;   /* keep the final x, v on the host for mdpd_server_get_state */
+    int32_t pad;
+} mdpd_job_spec;
+
+typedef struct mdpd_job_result {
+    int32_t state;        /* 0 queued, 1 running, 2 done, 3 failed, 4 cancelled */
+    int32_t error;        /* MDPD_* code when failed */
+    int64_t steps_done;
+    double submit_s, start_s, end_s;   /* host clock, seconds since server start */
+    double step_ms_p50, step_ms_p99;   /* per-step latency of this job while resident */
+    mdpd_thermo_t thermo;              /* at completion */
+} mdpd_job_result;
+
+/* device bytes a box of this spec holds while resident (the admission footprint) */
+int mdpd_box_bytes(const mdpd_box_spec *spec, uint64_t *bytes);
+int mdpd_server_start(mdpd_server_t **s, uint64_t budget_bytes, const mdpd_opts *opts);
+int mdpd_server_submit(mdpd_server_t *s, const mdpd_job_spec *job, int64_t *job_id);
+int mdpd_server_poll(mdpd_server_t *s, int64_t job_id, mdpd_job_result *out);
+int mdpd_server_get_state(mdpd_server_t *s, int64_t job_id, double *x, double *v, int64_t n);
+int mdpd_server_cancel(mdpd_server_t *s, int64_t job_id);
+/* wait until every submitted job is done, failed or cancelled (timeout_s <= 0: no limit) */
+int mdpd_server_drain(mdpd_server_t *s, double timeout_s);
+/* throughput/latency summary: particle-steps/s, step p50/p99 ms, job p50/p99 s,
+ * jobs done, peak resident bytes (7 doubles) */
+int mdpd_server_stats(mdpd_server_t *s, double *out7);
+void mdpd_server_stop(mdpd_server_t *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

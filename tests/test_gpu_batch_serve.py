@@ -1,0 +1,88 @@
+"""Batched and served boxes: each box's result is bitwise the same alone and in the mix
+(counter-based RNG, per-box deterministic lists and reductions); admission honours the
+HBM budget; failures of one job leave the others' results unchanged."""
+import time
+
+import numpy as np
+import pytest
+
+import mdpd
+
+pytestmark = pytest.mark.gpu
+
+
+def specs():
+    out = []
+    for k, (n, A, B, rd) in enumerate([(2200, -40, 25, 0.75), (7000, -45, 22, 0.72), (3300, -32, 28, 0.79),
+                                       (12000, -50, 20, 0.70)]):
+        L = (n / 6.05) ** (1 / 3)
+        out.append(mdpd.box_spec(n, L, A=A, B=B, cut_r=rd, seed=100 + k, init_seed=7 + k))
+    return out
+
+
+def run_alone(spec, steps):
+    b = mdpd.Batch([spec])
+    b.setup()
+    b.step(steps)
+    x, v = b.state(0)
+    t = b.thermo(0)
+    b.close()
+    return x, v, t
+
+
+def test_batch_equals_alone_bitwise():
+    sp = specs()
+    steps = 120
+    b = mdpd.Batch(sp)
+    b.setup()
+    b.step(steps)
+    for k, s in enumerate(sp):
+        xa, va, ta = run_alone(s, steps)
+        xb, vb = b.state(k)
+        assert np.array_equal(xa, xb) and np.array_equal(va, vb), k
+        assert b.thermo(k).nbuild == ta.nbuild
+    b.close()
+
+
+def test_server_continuous_batching_matches_alone():
+    sp = specs()
+    steps = [90, 150, 60, 120]
+    alone = [run_alone(s, n) for s, n in zip(sp, steps)]
+    # budget for the two largest boxes: later jobs wait for memory and join mid-run
+    foot = sorted(mdpd.box_bytes(s) for s in sp)
+    budget = foot[-1] + foot[-2] + 1024
+    srv = mdpd.Server(budget_bytes=budget)
+    ids = []
+    for s, n in zip(sp, steps):
+        ids.append(srv.submit(s, n, keep_state=True))
+        time.sleep(0.05)
+    srv.drain(timeout_s=300)
+    for k, jid in enumerate(ids):
+        r = srv.poll(jid)
+        assert r.state == 2 and r.steps_done == steps[k], (k, r.state, r.error)
+        x, v = srv.state(jid, sp[k].n)
+        assert np.array_equal(x, alone[k][0]) and np.array_equal(v, alone[k][1]), k
+        assert r.step_ms_p99 >= r.step_ms_p50 > 0
+    st = srv.stats()
+    assert st["jobs_done"] == len(ids)
+    assert st["peak_resident_bytes"] <= budget
+    srv.stop()
+
+
+def test_server_refuses_oversized_and_cancels():
+    srv = mdpd.Server(budget_bytes=int(5e8))
+    big = mdpd.box_spec(2_000_000, (2e6 / 6.05) ** (1 / 3))
+    with pytest.raises(mdpd.MdpdError) as e:
+        srv.submit(big, 10)
+    assert e.value.code == mdpd.ERR_BUDGET
+    sp = specs()
+    keep = srv.submit(sp[0], 40, keep_state=True)
+    gone = srv.submit(sp[1], 100000)
+    srv.cancel(gone)
+    srv.drain(timeout_s=120)
+    assert srv.poll(gone).state == 4
+    assert srv.poll(keep).state == 2
+    x, v = srv.state(keep, sp[0].n)
+    xa, va, _ = run_alone(sp[0], 40)
+    assert np.array_equal(x, xa) and np.array_equal(v, va)
+    srv.stop()

@@ -1,0 +1,270 @@
+"""Parity of the CUDA path with the oracle on the same seeded inputs (needs a B200).
+
+Tolerances (stated per result):
+  sort permutation, ghost images, pair sets, packed FP32 positions, RNG words: bit-exact
+  FP64 gaussian (parity mode): bit-exact;  FP32 gaussian: |err| <= 2e-6 (absolute)
+  density rho (FP32 pass vs FP64 oracle on the same list): <= 2e-6 relative
+  conservative forces at sigma = 0 (FP32 pass vs FP64 oracle): |df| <= 1e-5 * |F|_scale,
+  |F|_scale = sum over the particle's pairs of |F_ij| (the magnitude being summed)
+  full forces with the random term (exact RNG): same bound
+  one velocity-Verlet step (FP64 x, v from the same FP32 forces): bit-exact
+"""
+import os
+
+import numpy as np
+import pytest
+
+import mdpd
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def mdpd_box(n=6000, L=10.0, seed=4321, vseed=4928, kT=1.0, gamma=4.5, A=-40.0, B=25.0, rho_est=6.05,
+             exact=False, skin=0.3, extra=""):
+    lam = mdpd.Lammps()
+    lam.commands(f"""
+units lj
+dimension 3
+boundary p p p
+atom_style mdpd/atomic/meso {rho_est}
+neighbor {skin} bin
+neigh_modify every 1 delay 0 check yes
+region box block 0 {L} 0 {L} 0 {L} units box
+create_box 1 box
+create_atoms 1 random {n} {seed} box
+mass 1 1.0
+velocity all create 1.0 {vseed} dist gaussian
+pair_style mdpd/meso {kT} 1.0 123456
+pair_coeff 1 1 {A} {B} {gamma} 1.0 0.75
+pair_modify rng {'exact' if exact else 'fast'}
+fix BC all aboundary/rho/meso cut_rho 0.75
+fix NVE all nve/meso
+timestep 0.01
+run_style mvv/meso
+{extra}
+""")
+    return lam
+
+
+def dpd_box(n=3000, L=10.0, seed=777, vseed=999, exact=True):
+    lam = mdpd.Lammps()
+    lam.commands(f"""
+units lj
+atom_style dpd/atomic/meso
+neighbor 0.3 bin
+region box block 0 {L} 0 {L} 0 {L} units box
+create_box 1 box
+create_atoms 1 random {n} {seed} box
+mass 1 1.0
+velocity all create 1.0 {vseed}
+pair_style dpd/meso 1.0 5678
+pair_coeff 1 1 25.0 4.5 3.0 1.0
+pair_modify rng {'exact' if exact else 'fast'}
+fix NVE all nve/meso
+timestep 0.01
+run_style mvv/meso
+""")
+    return lam
+
+
+def oracle_rebuild(lam, L=10.0, rho_est=6.05):
+    x0, v0, tag0, typ0 = lam.state()  # tag order, before the device rebuild
+    return oracle.rebuild(x0, typ0, (0, 0, 0), (L, L, L), 1.0, 0.3, rho_est), x0, v0
+
+
+def test_sort_permutation_bit_exact():
+    lam = mdpd_box()
+    ref, _, _ = oracle_rebuild(lam)
+    lam.setup()
+    tags = lam.field("tag")
+    assert np.array_equal(tags, ref["tags"])
+    # wrapped FP64 positions in the new order are bit-identical
+    assert np.array_equal(lam.field("x").view(np.uint64), ref["x"].view(np.uint64))
+
+
+def test_ghost_images_and_packed_positions_bit_exact():
+    lam = mdpd_box()
+    ref, _, _ = oracle_rebuild(lam)
+    lam.setup()
+    g = lam.geometry()
+    n = lam.natoms()
+    assert g["nghost"] == len(ref["gsrc"])
+    tags = lam.field("tag")
+    gpu_set = set(zip(tags[lam.field("ghost_src")].tolist(), lam.field("ghost_img").tolist()))
+    ref_set = set(zip(ref["tags"][ref["gsrc"]].tolist(), ref["gimg"].tolist()))
+    assert gpu_set == ref_set
+    pos = lam.field("pos4")
+    assert np.array_equal(pos[:n, :3].view(np.uint32), ref["pos4"][:n, :3].view(np.uint32))
+    # ghost packed coordinates, matched by (source tag, image)
+    gk = {k: i for i, k in enumerate(zip(tags[lam.field("ghost_src")].tolist(), lam.field("ghost_img").tolist()))}
+    rk = list(zip(ref["tags"][ref["gsrc"]].tolist(), ref["gimg"].tolist()))
+    order = np.array([gk[k] for k in rk])
+    assert np.array_equal(pos[n + order, :3].view(np.uint32), ref["pos4"][n:, :3].view(np.uint32))
+
+
+@pytest.mark.parametrize("n,L", [(6000, 10.0), (20000, 15.0)])
+def test_pair_sets_bit_exact(n, L):
+    lam = mdpd_box(n=n, L=L)
+    ref, _, _ = oracle_rebuild(lam, L=L)
+    lam.setup()
+    ti, tj = lam.pairs()
+    ri, rj = oracle.pairs_from_rows(ref["count"], ref["table"], ref["tags"], ref["gsrc"])
+    a = np.sort(ti.astype(np.int64) * (1 << 32) + tj)
+    b = np.sort(ri.astype(np.int64) * (1 << 32) + rj)
+    assert len(a) == len(b)
+    assert np.array_equal(a, b)
+    assert len(np.unique(a)) == len(a)  # no duplicate images
+
+
+def test_rng_signatures_and_gaussian_bit_exact():
+    lam = mdpd_box()
+    lam.setup()
+    tags = lam.field("tag")
+    vel = lam.field("vel4")
+    sn = oracle.seed_now(123456, 0)
+    n = lam.natoms()
+    assert np.array_equal(vel[:n, 3].view(np.uint32), oracle.sig_mdpd(tags, sn))
+    rng = np.random.default_rng(11)
+    si = rng.integers(0, 2**32, 1 << 20, dtype=np.uint64).astype(np.uint32)
+    sj = rng.integers(0, 2**32, 1 << 20, dtype=np.uint64).astype(np.uint32)
+    si[:3] = [0, 0xFFFFFFFF, 1]; sj[:3] = [0, 0xFFFFFFFF, 0]
+    e, f = mdpd.gaussian(si, sj)
+    ref = oracle.gaussian(si, sj)
+    assert np.array_equal(e.view(np.uint64), ref.view(np.uint64))
+    assert np.max(np.abs(f.astype(np.float64) - ref)) <= 2e-6
+
+
+def test_gaussian_matches_reference_golden_when_present():
+    path = os.path.join(GOLDEN, "ref_device.json")
+    if not os.path.exists(path):
+        pytest.skip("no reference device vectors yet")
+    import json
+    g = json.load(open(path))
+    u = np.array(g["u"], np.uint32); v = np.array(g["v"], np.uint32)
+    ref = np.array([int(h, 16) for h in g["gauss"]], np.uint64)
+    e, _ = mdpd.gaussian(u, v)
+    assert np.array_equal(e.view(np.uint64), ref)
+
+
+def gpu_rows(lam):
+    cnt, rows = lam.list_rows()
+    return cnt, np.where(rows < 0, 0, rows).astype(np.int32)
+
+
+def test_density_matches_oracle():
+    lam = mdpd_box()
+    lam.setup()
+    n = lam.natoms()
+    cnt, rows = gpu_rows(lam)
+    pos = lam.field("pos4")
+    rho = lam.field("rho")
+    ref = oracle.density(pos, cnt, rows, np.ones(n, np.int32), 1, 0.75, np.ones(8))
+    assert np.max(np.abs(rho[:n] - ref) / ref) < 2e-6
+
+
+def force_scale(pos, cnt, rows, coeffs, rho, n):
+    # sum_j |F_ij| per particle (conservative part), the size of the terms the pass sums
+    s = np.zeros(n)
+    c = coeffs[(0, 0)]
+    for i in range(n):
+        js = rows[i, :cnt[i]]
+        d = pos[i, :3].astype(np.float64) - pos[js, :3].astype(np.float64)
+        r = np.sqrt((d * d).sum(1))
+        m = (r < c[0]) & (r > 1e-10)
+        wc = 1 - r[m] / c[0]
+        wr = np.maximum(1 - r[m] / c[1], 0)
+        s[i] = np.abs(c[2] * wc + c[3] * (rho[i] + rho[js[m]]) * wr).sum()
+    return s
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_conservative_force_sigma0(exact):
+    lam = mdpd_box(kT=0.0, gamma=0.0, exact=exact)
+    lam.setup()
+    n = lam.natoms()
+    cnt, rows = gpu_rows(lam)
+    pos, vel, rho = lam.field("pos4"), lam.field("vel4"), lam.field("rho").astype(np.float64)
+    f = lam.field("force")[:, :3].astype(np.float64)
+    coeffs = {(0, 0): (1.0, 0.75, -40.0, 25.0, 0.0, 0.0)}
+    ref = oracle.force_mdpd(pos, vel, rho, cnt, rows, coeffs, 0.01)
+    scale = force_scale(pos, cnt, rows, coeffs, rho, n)
+    err = np.abs(f - ref).max(1)
+    assert np.all(err <= 1e-5 * scale + 1e-6), (err / scale).max()
+
+
+def test_full_force_with_exact_rng():
+    lam = mdpd_box(exact=True)
+    lam.setup()
+    n = lam.natoms()
+    cnt, rows = gpu_rows(lam)
+    pos, vel, rho = lam.field("pos4"), lam.field("vel4"), lam.field("rho").astype(np.float64)
+    f = lam.field("force")[:, :3].astype(np.float64)
+    sigma = np.sqrt(2 * 1.0 * 4.5)
+    coeffs = {(0, 0): (1.0, 0.75, -40.0, 25.0, 4.5, sigma)}
+    ref = oracle.force_mdpd(pos, vel, rho, cnt, rows, coeffs, 0.01)
+    scale = force_scale(pos, cnt, rows, coeffs, rho, n) + np.abs(ref).max(1)
+    err = np.abs(f - ref).max(1)
+    assert np.all(err <= 1e-5 * scale + 1e-5), (err / scale).max()
+
+
+def test_velocity_verlet_step_bit_exact():
+    lam = mdpd_box()
+    lam.setup()
+    x0 = lam.field("x"); tags = lam.field("tag")
+    f0 = lam.field("force")[:, :3].astype(np.float64)
+    _, v0s, _, _ = lam.state()  # tag order
+    v0 = v0s[tags - 1]
+    lam.step(1)
+    assert np.array_equal(lam.field("tag"), tags)  # no rebuild on the first step at T=1
+    x1 = lam.field("x")
+    fma = oracle.lib().orc_fma
+    dtfm = 0.5 * 0.01 * oracle.lib().orc_rcp(1.0)
+    for i in range(0, len(x0), 97):
+        for d in range(3):
+            vh = fma(dtfm, f0[i, d], v0[i, d])
+            assert x1[i, d] == fma(0.01, vh, x0[i, d])
+
+
+def test_dpd_pairs_signatures_and_forces():
+    lam = dpd_box()
+    x0, _, _, typ0 = lam.state()
+    ref = oracle.rebuild(x0, typ0, (0, 0, 0), (10, 10, 10), 1.0, 0.3, 0.0)
+    lam.setup()
+    assert np.array_equal(lam.field("tag"), ref["tags"])
+    ti, tj = lam.pairs()
+    ri, rj = oracle.pairs_from_rows(ref["count"], ref["table"], ref["tags"], ref["gsrc"])
+    assert np.array_equal(np.sort(ti.astype(np.int64) * (1 << 32) + tj), np.sort(ri.astype(np.int64) * (1 << 32) + rj))
+    n = lam.natoms()
+    vel = lam.field("vel4")
+    sn = oracle.seed_now(5678, 0)
+    assert np.array_equal(vel[:n, 3].view(np.uint32), oracle.sig_dpd(lam.field("tag"), vel[:n], sn))
+    cnt, rows = gpu_rows(lam)
+    pos = lam.field("pos4")
+    f = lam.field("force")[:, :3].astype(np.float64)
+    reff = oracle.force_dpd(pos, vel, cnt, rows, {(0, 0): (1.0, 25.0, 4.5, 3.0, 1.0)}, 0.01)
+    scale = np.abs(reff).max(1) + 25.0
+    assert np.all(np.abs(f - reff).max(1) <= 1e-5 * scale)
+
+
+def test_list_overflow_reported_not_crashed():
+    # a density estimate far below the real density gives too short rows (n_col = 32):
+    # the build stops inserting at the row end and the call returns MDPD_ERR_OVERFLOW
+    lam = mdpd_box(rho_est=0.1)
+    with pytest.raises(mdpd.MdpdError) as e:
+        lam.setup()
+    assert e.value.code == mdpd.ERR_OVERFLOW
+
+
+def test_deterministic_replay():
+    out = []
+    for _ in range(2):
+        lam = mdpd_box(n=4000)
+        lam.setup()
+        lam.step(50)
+        x, v, _, _ = lam.state()
+        out.append((x, v))
+        lam.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])

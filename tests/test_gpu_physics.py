@@ -1,0 +1,156 @@
+"""Statistical checks of whole runs on the GPU against the reference's decks and the oracle.
+
+Tolerances: temperature within 1% of the thermostat value in long runs (fluctuation-
+averaged), density profiles within 2% in the bulk bins of the reference's own deck output,
+momentum conserved to 1e-9 per particle (pairwise forces and noise are antisymmetric).
+"""
+import gzip
+import json
+import os
+import shutil
+
+import numpy as np
+import pytest
+
+import mdpd
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_dpd_config1_temperature_and_momentum(tmp_path):
+    # classic DPD fluid: 10^3 box, rho = 3, a = 25, gamma = 4.5, sigma = 3, dt = 0.01
+    lam = mdpd.Lammps()
+    lam.commands("""
+units lj
+atom_style dpd/atomic/meso
+neighbor 0.3 bin
+region box block 0 10 0 10 0 10 units box
+create_box 1 box
+create_atoms 1 random 3000 87287 box
+mass 1 1.0
+velocity all create 1.0 4928459
+pair_style dpd/meso 1.0 34387
+pair_coeff 1 1 25.0 4.5 3.0 1.0
+fix NVE all nve/meso
+timestep 0.01
+run_style mvv/meso
+thermo 100
+""")
+    lam.run(200)
+    temps = []
+    for _ in range(16):
+        lam.run(50)
+        temps.append(lam.thermo().temp)
+    t = lam.thermo()
+    assert abs(np.mean(temps) - 1.0) < 0.02
+    assert np.max(np.abs(t.momentum)) < 1e-9 * 3000
+    assert "Step Temp" in lam.log
+
+
+def test_mdpd_liquid_temperature_and_density():
+    lam = mdpd.Lammps()
+    lam.commands("""
+units lj
+atom_style mdpd/atomic/meso 6.05
+neighbor 0.3 bin
+region box block 0 12 0 12 0 12 units box
+create_box 1 box
+create_atoms 1 random 10454 2323 box
+mass 1 1.0
+velocity all create 1.0 77
+pair_style mdpd/meso 1.0 1.0 9876
+pair_coeff 1 1 -40 25 4.5 1.0 0.75
+fix BC all aboundary/rho/meso cut_rho 0.75
+fix NVE all nve/meso
+timestep 0.01
+run_style mvv/meso
+thermo 1000
+""")
+    lam.run(1000)
+    temps = []
+    for _ in range(20):
+        lam.run(50)
+        temps.append(lam.thermo().temp)
+    assert abs(np.mean(temps) - 1.0) < 0.01
+    rho = lam.field("rho")[: lam.natoms()]
+    assert np.isfinite(rho).all() and 5.0 < rho.mean() < 12.0
+
+
+def test_static_contact_angle_deck(tmp_path):
+    """examples/v2.5/static_contact_angle_in_a_slit_nano_channel with A_SL = -30: the
+    10-bin y density profile of the 4,000 fluid particles against the reference's own
+    GPU output out.profile.a_-30 (reference run: 5,000 + 100,000 steps)."""
+    data = tmp_path / "LAMMPS_init_noimage.dat"
+    with gzip.open(os.path.join(GOLDEN, "static_contact_init.dat.gz"), "rb") as f, open(data, "wb") as g:
+        shutil.copyfileobj(f, g)
+    nsteps = int(os.environ.get("MDPD_STATIC_CONTACT_STEPS", "100000"))
+    out = tmp_path / "out.profile"
+    lam = mdpd.Lammps()
+    lam.commands(f"""
+variable kBT equal 1.0
+variable cut_att equal 1.00
+variable cut_rep equal 0.75
+variable cut_rho equal 0.75
+variable cut_phi equal 1.00
+variable skin equal 0.3*${{cut_att}}
+variable rho_solids equal 8.0
+units lj
+dimension 3
+boundary p p p
+neighbor ${{skin}} bin
+neigh_modify every 1 delay 0 check yes
+atom_style mdpd/atomic/meso 3
+read_data {data}
+group group_fluid1 type 1
+group group_solid2 type 2
+pair_style mdpd/meso ${{kBT}} ${{cut_att}} 123456 group_fluid1 group_solid2
+pair_coeff 1 1 -40 25 18.0 ${{cut_att}} ${{cut_rep}}
+pair_coeff 1 2 -30 25 18.0 ${{cut_att}} ${{cut_rep}}
+pair_coeff 2 2 -40 25 18.0 ${{cut_att}} ${{cut_rep}}
+mass 1 1
+mass 2 1
+timestep 0.01
+fix BC all aboundary/rho/meso cut_rho ${{cut_rho}} phi_c 0.5 cut_phi ${{cut_phi}} rho_wall ${{rho_solids}} wall group_solid2 mobile group_fluid1
+thermo 1000
+fix int_f group_fluid1 nve/meso
+run_style mvv/meso
+run 5000
+reset_timestep 0
+fix dn group_fluid1 density/meso along y nbin 10 every 99999 window 99998 output {out}
+""")
+    lam.run(nsteps)
+    lam.close()  # the fix writes its open window at destruction
+    files = sorted(p for p in os.listdir(tmp_path) if p.startswith("out.profile."))
+    assert files, os.listdir(tmp_path)
+    prof = np.loadtxt(tmp_path / files[-1])
+    ref = np.array(json.load(open(os.path.join(GOLDEN, "static_contact_profiles.json")))["gpu"]["-30"])
+    assert np.allclose(prof[:, 0], ref[:, 0])
+    assert abs(prof[:, 1].sum() - 4000) < 1.0
+    bulk = slice(2, 8)
+    rel = np.abs(prof[bulk, 1] - ref[bulk, 1]) / ref[bulk, 1]
+    tol = 0.02 if nsteps >= 100000 else 0.05
+    assert np.all(rel < tol), (prof[:, 1], ref[:, 1])
+    # wall-adjacent bins and the empty wall bins
+    assert np.all(np.abs(prof[[1, 8], 1] - ref[[1, 8], 1]) / ref[[1, 8], 1] < 2 * tol)
+    assert prof[0, 1] < 1.0 and prof[9, 1] < 1.0
+
+
+def test_gpu_temperature_agrees_with_oracle_engine():
+    # same initial state through the GPU path and the FP64 oracle engine: ensemble averages agree
+    rng = np.random.default_rng(5)
+    n, L = 3000, 10.0
+    x = rng.uniform(0, L, (n, 3))
+    v = rng.normal(0, 1, (n, 3)); v -= v.mean(0)
+    spec = mdpd.box_spec(n, L, style=1, A=25.0, gamma=4.5, sigma=3.0, rho_est=0.0, seed=99, x=x, v=v, exact_rng=1)
+    b = mdpd.Batch([spec])
+    b.setup()
+    sim = oracle.Sim(x, v, (0, 0, 0), (L, L, L), style=1, a0=25.0, gamma=4.5, sigma=3.0, seed=99, rho_est=0.0)
+    sim.setup()
+    tg, to = [], []
+    for _ in range(10):
+        b.step(30); sim.run(30)
+        tg.append(b.thermo(0).temp); to.append(sim.thermo()["temp"])
+    assert abs(np.mean(tg) - np.mean(to)) < 0.03

@@ -1,0 +1,565 @@
+// extern "C" entry points of libmdpd.so (include/mdpd.h).  Exceptions never cross the
+// boundary: each call maps them to an MDPD_* status and keeps the message for
+// mdpd_last_error.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/mdpd.h"
+#include "engine.h"
+#include "script.h"
+
+using namespace mdpd;
+
+struct mdpd_s {
+    std::unique_ptr<Script> script;
+    std::string err;
+    int verbose = 0;
+};
+
+struct mdpd_batch_s {
+    std::vector<std::unique_ptr<Box>> boxes;
+    std::unique_ptr<Batch> batch;
+    std::string err;
+};
+
+static thread_local std::string g_err;
+
+static int code_of(const std::string &m)
+{
+    if (m.rfind("OOM", 0) == 0) return MDPD_ERR_OOM;
+    if (m.rfind("ARG", 0) == 0) return MDPD_ERR_ARG;
+    if (m.rfind("PARSE", 0) == 0) return MDPD_ERR_PARSE;
+    if (m.rfind("CUDA", 0) == 0) return MDPD_ERR_CUDA;
+    if (m.rfind("BUDGET", 0) == 0) return MDPD_ERR_BUDGET;
+    return MDPD_ERR_STATE;
+}
+
+template <class F> static int guard(std::string &err, F &&f)
+{
+    try {
+        f();
+        err.clear();
+        return MDPD_OK;
+    } catch (const ScriptError &e) {
+        err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        err = "host allocation failed";
+        return MDPD_ERR_OOM;
+    } catch (const std::exception &e) {
+        err = e.what();
+        return code_of(err);
+    }
+}
+
+static void fill_thermo(const Thermo &t, mdpd_thermo_t *o)
+{
+    std::memset(o, 0, sizeof(*o));
+    o->step = t.step;
+    o->natoms = t.n;
+    o->nbuild = t.nbuild;
+    o->temp = t.temp;
+    o->press = t.press;
+    o->pe = t.pe;
+    o->ke = 0.5 * t.ke_all;
+    for (int k = 0; k < 6; ++k) o->virial[k] = t.virial[k];
+    for (int k = 0; k < 3; ++k) o->momentum[k] = t.mom[k];
+    o->temp_group = t.n_group > 1 ? t.ke_group / (3.0 * t.n_group - 3.0) : 0.0;
+    o->status = t.status;
+}
+
+extern "C" {
+
+int mdpd_create(mdpd_t **h, const mdpd_opts *opts)
+{
+    if (!h) return MDPD_ERR_ARG;
+    *h = nullptr;
+    std::unique_ptr<mdpd_s> s(new mdpd_s);
+    const int rc = guard(g_err, [&] { s->script.reset(new Script(opts ? opts->device : 0)); });
+    if (rc) return rc;
+    s->verbose = opts ? opts->verbose : 0;
+    *h = s.release();
+    return MDPD_OK;
+}
+
+int mdpd_command(mdpd_t *h, const char *line)
+{
+    if (!h || !line) return MDPD_ERR_ARG;
+    return guard(h->err, [&] { h->script->command(line); });
+}
+
+int mdpd_file(mdpd_t *h, const char *path)
+{
+    if (!h || !path) return MDPD_ERR_ARG;
+    return guard(h->err, [&] { h->script->file(path); });
+}
+
+int mdpd_run(mdpd_t *h, int64_t nsteps)
+{
+    if (!h || nsteps < 0) return MDPD_ERR_ARG;
+    return guard(h->err, [&] { h->script->run(nsteps); });
+}
+
+int mdpd_setup(mdpd_t *h)
+{
+    if (!h) return MDPD_ERR_ARG;
+    return guard(h->err, [&] { h->script->setup(); });
+}
+
+int mdpd_step(mdpd_t *h, int64_t nsteps)
+{
+    if (!h || nsteps < 0) return MDPD_ERR_ARG;
+    return guard(h->err, [&] {
+        Batch *b = h->script->batch();
+        if (!b || !h->script->box()) throw ScriptError(MDPD_ERR_STATE, "mdpd_step before mdpd_setup/mdpd_run");
+        b->run(nsteps, true);
+        std::string msg;
+        if (int st = b->status(msg)) throw ScriptError(st & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, msg);
+    });
+}
+
+int mdpd_natoms(mdpd_t *h, int64_t *n)
+{
+    if (!h || !n) return MDPD_ERR_ARG;
+    *n = (int64_t)h->script->particles().size();
+    return MDPD_OK;
+}
+
+int mdpd_get_state(mdpd_t *h, double *x, double *v, int32_t *tag, int32_t *type, int64_t n)
+{
+    if (!h) return MDPD_ERR_ARG;
+    return guard(h->err, [&] {
+        h->script->sync_host();
+        Particles &p = h->script->particles();
+        if ((int64_t)p.size() != n) throw ScriptError(MDPD_ERR_ARG, "size mismatch");
+        // parts_ is in tag order after setup; sort defensively
+        std::vector<size_t> ord(p.size());
+        for (size_t i = 0; i < ord.size(); ++i) ord[i] = i;
+        std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return p.tag[a] < p.tag[b]; });
+        for (size_t r = 0; r < ord.size(); ++r) {
+            const size_t i = ord[r];
+            for (int d = 0; d < 3; ++d) {
+                if (x) x[3 * r + d] = p.x[3 * i + d];
+                if (v) v[3 * r + d] = p.v[3 * i + d];
+            }
+            if (tag) tag[r] = p.tag[i];
+            if (type) type[r] = p.type[i];
+        }
+    });
+}
+
+int mdpd_set_state(mdpd_t *h, const double *x, const double *v, int64_t n)
+{
+    if (!h) return MDPD_ERR_ARG;
+    return guard(h->err, [&] {
+        h->script->sync_host();
+        Particles &p = h->script->particles();
+        if ((int64_t)p.size() != n) throw ScriptError(MDPD_ERR_ARG, "size mismatch");
+        for (size_t i = 0; i < p.size(); ++i) {
+            const int64_t r = p.tag[i] - 1;
+            if (r < 0 || r >= n) throw ScriptError(MDPD_ERR_ARG, "tags must be 1..n");
+            for (int d = 0; d < 3; ++d) {
+                if (x) p.x[3 * i + d] = x[3 * r + d];
+                if (v) p.v[3 * i + d] = v[3 * r + d];
+            }
+        }
+        h->script->invalidate();
+    });
+}
+
+int mdpd_thermo(mdpd_t *h, mdpd_thermo_t *out)
+{
+    if (!h || !out) return MDPD_ERR_ARG;
+    return guard(h->err, [&] {
+        Thermo t;
+        h->script->thermo(t);
+        fill_thermo(t, out);
+    });
+}
+
+const char *mdpd_log(mdpd_t *h) { return h ? h->script->log.c_str() : ""; }
+const char *mdpd_last_error(mdpd_t *h) { return h ? h->err.c_str() : g_err.c_str(); }
+
+void mdpd_destroy(mdpd_t *h)
+{
+    if (!h) return;
+    try {
+        h->script.reset();
+    } catch (...) {
+    }
+    delete h;
+}
+
+// --- internal arrays --------------------------------------------------------------------
+
+static int64_t field_count(Box &b, const std::string &name)
+{
+    BoxState st = b.state();
+    st.nghost = std::min(st.nghost, b.desc.ghost_cap);
+    const int64_t n = b.n, na = (int64_t)b.n + st.nghost;
+    if (name == "pos4" || name == "vel4") return 4 * na;
+    if (name == "rho") return na;
+    if (name == "force") return 4 * n;
+    if (name == "count" || name == "tag" || name == "type" || name == "mask") return n;
+    if (name == "ghost_src" || name == "ghost_img") return st.nghost;
+    if (name == "x" || name == "v") return 3 * n;
+    if (name == "list") return (int64_t)b.desc.nrow * b.desc.n_col;
+    throw ScriptError(MDPD_ERR_ARG, "unknown field " + name);
+}
+
+int mdpd_field_size(mdpd_t *h, const char *name, int64_t *count)
+{
+    if (!h || !name || !count) return MDPD_ERR_ARG;
+    return guard(h->err, [&] {
+        Box *b = h->script->box();
+        if (!b) throw ScriptError(MDPD_ERR_STATE, "no device state");
+        *count = field_count(*b, name);
+    });
+}
+
+int mdpd_get_field(mdpd_t *h, const char *name, void *out, int64_t nbytes)
+{
+    if (!h || !name || !out) return MDPD_ERR_ARG;
+    return guard(h->err, [&] {
+        Box *b = h->script->box();
+        if (!b) throw ScriptError(MDPD_ERR_STATE, "no device state");
+        const std::string f = name;
+        const int64_t cnt = field_count(*b, f);
+        const BoxState st = b->state();
+        const BoxDesc &B = b->desc;
+        const int c = st.cur;
+        auto get = [&](const void *src, size_t esz) {
+            if ((int64_t)(cnt * esz) > nbytes) throw ScriptError(MDPD_ERR_ARG, "buffer too small");
+            check_cuda(cudaMemcpy(out, src, cnt * esz, cudaMemcpyDeviceToHost), "get field");
+        };
+        if (f == "pos4") get(B.pos, 4);
+        else if (f == "vel4") get(B.vel, 4);
+        else if (f == "rho") get(B.rho, 4);
+        else if (f == "force") get(B.f[c], 4);
+        else if (f == "count") get(B.count, 4);
+        else if (f == "tag") get(B.tag[c], 4);
+        else if (f == "type") get(B.type[c], 4);
+        else if (f == "mask") get(B.mask[c], 4);
+        else if (f == "ghost_src") get(B.gsrc, 4);
+        else if (f == "ghost_img") get(B.gimg, 4);
+        else if (f == "list") get(B.table, 4);
+        else if (f == "x" || f == "v") {
+            if (cnt * 8 > nbytes) throw ScriptError(MDPD_ERR_ARG, "buffer too small");
+            if (f == "x") b->download_state((double *)out, nullptr, nullptr, nullptr, nullptr, nullptr);
+            else b->download_state(nullptr, (double *)out, nullptr, nullptr, nullptr, nullptr);
+        }
+    });
+}
+
+int mdpd_geometry(mdpd_t *h, double *o)
+{
+    if (!h || !o) return MDPD_ERR_ARG;
+    return guard(h->err, [&] {
+        Box *b = h->script->box();
+        if (!b) throw ScriptError(MDPD_ERR_STATE, "no device state");
+        const BoxState st = b->state();
+        const BoxDesc &B = b->desc;
+        for (int d = 0; d < 3; ++d) {
+            o[d] = B.lo[d];
+            o[3 + d] = B.hi[d];
+            o[6 + d] = B.cen[d];
+            o[9 + d] = B.mbin[d];
+        }
+        o[12] = B.cutghost;
+        o[13] = B.n_col;
+        o[14] = st.nghost;
+        // n_bulk and nbuild are readable through mdpd_thermo / fields
+    });
+}
+
+int mdpd_get_pairs(mdpd_t *h, int32_t *ti, int32_t *tj, int64_t cap, int64_t *npairs)
+{
+    if (!h || !npairs) return MDPD_ERR_ARG;
+    return guard(h->err, [&] {
+        Box *b = h->script->box();
+        if (!b) throw ScriptError(MDPD_ERR_STATE, "no device state");
+        BoxState st = b->state();
+        const BoxDesc &B = b->desc;
+        st.nghost = std::min(st.nghost, B.ghost_cap);
+        const int n = b->n, c = st.cur;
+        std::vector<int> cnt(n), tag(n), gsrc(std::max(st.nghost, 1));
+        std::vector<int> table((size_t)B.nrow * B.n_col);
+        check_cuda(cudaMemcpy(cnt.data(), B.count, 4 * n, cudaMemcpyDeviceToHost), "pairs");
+        check_cuda(cudaMemcpy(tag.data(), B.tag[c], 4 * n, cudaMemcpyDeviceToHost), "pairs");
+        if (st.nghost) check_cuda(cudaMemcpy(gsrc.data(), B.gsrc, 4 * st.nghost, cudaMemcpyDeviceToHost), "pairs");
+        check_cuda(cudaMemcpy(table.data(), B.table, 4 * table.size(), cudaMemcpyDeviceToHost), "pairs");
+        int64_t np = 0;
+        for (int i = 0; i < n; ++i)
+            for (int k = 0; k < cnt[i]; ++k) {
+                const int j = table[(size_t)((i & ~31) + (k & 31)) * B.n_col + (k & ~31) + (i & 31)];
+                if (np < cap && ti && tj) {
+                    ti[np] = tag[i];
+                    tj[np] = j < n ? tag[j] : tag[gsrc[j - n]];
+                }
+                ++np;
+            }
+        *npairs = np;
+    });
+}
+
+int mdpd_gaussian(const uint32_t *si, const uint32_t *sj, double *exact, float *fast, int64_t n)
+{
+    if (!si || !sj || n < 0) return MDPD_ERR_ARG;
+    return guard(g_err, [&] {
+        if (n == 0) return;
+        uint32_t *d_i, *d_j;
+        double *d_e = nullptr;
+        float *d_f = nullptr;
+        check_cuda(cudaMalloc(&d_i, 4 * n), "gaussian");
+        check_cuda(cudaMalloc(&d_j, 4 * n), "gaussian");
+        if (exact) check_cuda(cudaMalloc(&d_e, 8 * n), "gaussian");
+        if (fast) check_cuda(cudaMalloc(&d_f, 4 * n), "gaussian");
+        check_cuda(cudaMemcpy(d_i, si, 4 * n, cudaMemcpyHostToDevice), "gaussian");
+        check_cuda(cudaMemcpy(d_j, sj, 4 * n, cudaMemcpyHostToDevice), "gaussian");
+        launch_gaussian(0, d_i, d_j, d_e, d_f, (int)n);
+        check_cuda(cudaGetLastError(), "gaussian launch");
+        if (exact) check_cuda(cudaMemcpy(exact, d_e, 8 * n, cudaMemcpyDeviceToHost), "gaussian");
+        if (fast) check_cuda(cudaMemcpy(fast, d_f, 4 * n, cudaMemcpyDeviceToHost), "gaussian");
+        cudaFree(d_i);
+        cudaFree(d_j);
+        cudaFree(d_e);
+        cudaFree(d_f);
+    });
+}
+
+// --- batch ------------------------------------------------------------------------------
+
+}  // extern "C"
+
+namespace mdpd {
+
+// synthetic box of a mdpd_box_spec: the physics and, if x is NULL, a seeded uniform fill
+void spec_from_box(const mdpd_box_spec &bs, Spec &s, Particles &p)
+{
+    if (bs.n <= 0) throw std::runtime_error("ARG: box spec with n <= 0");
+    s = Spec();
+    s.style = bs.style;
+    s.ntype = 1;
+    for (int d = 0; d < 3; ++d) s.lo[d] = bs.lo[d], s.hi[d] = bs.hi[d];
+    s.skin = bs.skin > 0 ? bs.skin : 0.3;
+    s.every = bs.every > 0 ? bs.every : 1;
+    s.delay = bs.delay;
+    s.check = bs.check;
+    s.dt = bs.dt > 0 ? bs.dt : 0.01;
+    s.kT = bs.kT;
+    s.seed = bs.seed;
+    s.rho_est = bs.rho_est;
+    s.mass[0] = bs.mass > 0 ? bs.mass : 1.0;
+    s.cut_rho = bs.cut_rho > 0 ? bs.cut_rho : 0.75;
+    s.exact_rng = bs.exact_rng;
+    PairParam q;
+    q.set = 1;
+    q.A = bs.A, q.B = bs.B, q.gamma = bs.gamma, q.cut = bs.cut > 0 ? bs.cut : 1.0;
+    q.cut_r = bs.cut_r > 0 ? bs.cut_r : 0.75;
+    q.sigma = bs.sigma;
+    q.expw = 1.0;
+    if (q.cut < q.cut_r) throw std::runtime_error("PARSE: cutA should be larger than cutB.");
+    s.pair[0][0] = q;
+    const int n = bs.n;
+    p = Particles();
+    p.x.resize(3 * (size_t)n);
+    p.v.resize(3 * (size_t)n);
+    p.tag.resize(n);
+    p.type.assign(n, 1);
+    p.mask.assign(n, 1);
+    for (int i = 0; i < n; ++i) p.tag[i] = i + 1;
+    if (bs.x) {
+        std::copy(bs.x, bs.x + 3 * (size_t)n, p.x.begin());
+        if (bs.v) std::copy(bs.v, bs.v + 3 * (size_t)n, p.v.begin());
+        return;
+    }
+    std::mt19937_64 rng(bs.init_seed);
+    std::uniform_real_distribution<double> u(0.0, 1.0);
+    std::normal_distribution<double> g(0.0, 1.0);
+    double flo[3], fhi[3];
+    for (int d = 0; d < 3; ++d) {
+        const bool sub = bs.fill_hi[d] > bs.fill_lo[d];
+        flo[d] = sub ? std::max(bs.fill_lo[d], bs.lo[d]) : bs.lo[d];
+        fhi[d] = sub ? std::min(bs.fill_hi[d], bs.hi[d]) : bs.hi[d];
+    }
+    const double sv = std::sqrt(bs.kT / s.mass[0]);
+    double mom[3] = {0, 0, 0};
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            double x = flo[d] + u(rng) * (fhi[d] - flo[d]);
+            if (x >= bs.hi[d]) x = bs.lo[d];
+            p.x[3 * i + d] = x;
+            p.v[3 * i + d] = sv * g(rng);
+            mom[d] += p.v[3 * i + d];
+        }
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) p.v[3 * i + d] -= mom[d] / n;
+}
+
+}  // namespace mdpd
+
+extern "C" {
+
+int mdpd_batch_create(mdpd_batch_t **out, const mdpd_box_spec *specs, int32_t nbox, const mdpd_opts *opts)
+{
+    if (!out || !specs || nbox <= 0) return MDPD_ERR_ARG;
+    *out = nullptr;
+    std::unique_ptr<mdpd_batch_s> b(new mdpd_batch_s);
+    const int rc = guard(g_err, [&] {
+        check_cuda(cudaSetDevice(opts ? opts->device : 0), "set device");
+        StepConfig cfg;
+        cfg.sms = sm_count();
+        cfg.style = specs[0].style;
+        cfg.exact_rng = specs[0].exact_rng;
+        std::vector<Box *> raw;
+        for (int k = 0; k < nbox; ++k) {
+            if (specs[k].style != cfg.style) throw std::runtime_error("ARG: a batch holds boxes of one pair style");
+            Spec s;
+            Particles p;
+            spec_from_box(specs[k], s, p);
+            b->boxes.emplace_back(new Box(s, p, cfg.sms));
+            raw.push_back(b->boxes.back().get());
+        }
+        b->batch.reset(new Batch(raw, cfg));
+    });
+    if (rc) return rc;
+    *out = b.release();
+    return MDPD_OK;
+}
+
+int mdpd_batch_setup(mdpd_batch_t *b)
+{
+    if (!b) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        b->batch->setup();
+        std::string msg;
+        if (int st = b->batch->status(msg)) throw ScriptError(st & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, msg);
+    });
+}
+
+int mdpd_batch_step(mdpd_batch_t *b, int64_t nsteps)
+{
+    if (!b || nsteps < 0) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        b->batch->run(nsteps, true);
+        std::string msg;
+        if (int st = b->batch->status(msg)) throw ScriptError(st & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, msg);
+    });
+}
+
+int mdpd_batch_thermo(mdpd_batch_t *b, int32_t box, mdpd_thermo_t *out)
+{
+    if (!b || !out || box < 0 || box >= (int)b->boxes.size()) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        std::vector<Thermo> t;
+        b->batch->thermo(t);
+        fill_thermo(t[box], out);
+    });
+}
+
+int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int64_t n)
+{
+    if (!b || box < 0 || box >= (int)b->boxes.size()) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        Box &bx = *b->boxes[box];
+        if (n != bx.n) throw ScriptError(MDPD_ERR_ARG, "size mismatch");
+        std::vector<double> xi(3 * (size_t)n), vi(3 * (size_t)n);
+        std::vector<int32_t> tag(n);
+        bx.download_state(xi.data(), vi.data(), nullptr, tag.data(), nullptr, nullptr);
+        for (int i = 0; i < n; ++i) {
+            const int r = tag[i] - 1;
+            for (int d = 0; d < 3; ++d) {
+                if (x) x[3 * r + d] = xi[3 * i + d];
+                if (v) v[3 * r + d] = vi[3 * i + d];
+            }
+        }
+    });
+}
+
+int mdpd_batch_time(mdpd_batch_t *b, int64_t nsteps, double *ms)
+{
+    if (!b || !ms || nsteps <= 0) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        cudaEvent_t e0, e1;
+        check_cuda(cudaEventCreate(&e0), "event");
+        check_cuda(cudaEventCreate(&e1), "event");
+        cudaStream_t s = b->batch->stream();
+        check_cuda(cudaEventRecord(e0, s), "event");
+        b->batch->run(nsteps, false);
+        check_cuda(cudaEventRecord(e1, s), "event");
+        check_cuda(cudaEventSynchronize(e1), "event");
+        float t = 0;
+        check_cuda(cudaEventElapsedTime(&t, e0, e1), "event");
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms = t / nsteps;
+        std::string msg;
+        if (int st = b->batch->status(msg)) throw ScriptError(st & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, msg);
+    });
+}
+
+int mdpd_batch_tune(mdpd_batch_t *b, int32_t *tpp_density, int32_t *tpp_force)
+{
+    if (!b) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        const StepConfig base = b->batch->cfg;
+        double best = 1e30;
+        StepConfig pick = base;
+        for (int td : {1, 2, 4})
+            for (int tf : {1, 2, 4}) {
+                StepConfig c = base;
+                c.tpp_density = td;
+                c.tpp_force = tf;
+                b->batch->reconfigure(c);
+                b->batch->run(3, true);
+                cudaEvent_t e0, e1;
+                cudaEventCreate(&e0);
+                cudaEventCreate(&e1);
+                cudaEventRecord(e0, b->batch->stream());
+                b->batch->run(10, false);
+                cudaEventRecord(e1, b->batch->stream());
+                cudaEventSynchronize(e1);
+                float t = 0;
+                cudaEventElapsedTime(&t, e0, e1);
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                if (t < best) best = t, pick = c;
+            }
+        b->batch->reconfigure(pick);
+        if (tpp_density) *tpp_density = pick.tpp_density;
+        if (tpp_force) *tpp_force = pick.tpp_force;
+    });
+}
+
+int mdpd_batch_profile(mdpd_batch_t *b, int64_t nsteps, double *out5)
+{
+    if (!b || !out5 || nsteps <= 0) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        b->batch->profile(nsteps, out5);
+        std::string msg;
+        if (int st = b->batch->status(msg)) throw ScriptError(st & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, msg);
+    });
+}
+
+int mdpd_batch_rebuild_steps(mdpd_batch_t *b, int64_t *n)
+{
+    if (!b || !n) return MDPD_ERR_ARG;
+    return guard(b->err, [&] { *n = b->batch->rebuild_steps(); });
+}
+
+const char *mdpd_batch_last_error(mdpd_batch_t *b) { return b ? b->err.c_str() : g_err.c_str(); }
+
+void mdpd_batch_destroy(mdpd_batch_t *b)
+{
+    if (!b) return;
+    b->batch.reset();
+    b->boxes.clear();
+    delete b;
+}
+
+}  // extern "C"

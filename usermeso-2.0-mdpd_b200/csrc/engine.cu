@@ -1,0 +1,562 @@
+// Host runtime: device allocation of boxes, the per-step CUDA graph (integrate ->
+// IF(rebuild){...} -> density -> force), setup and thermo.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <stdexcept>
+
+namespace mdpd {
+
+std::string cuda_err(cudaError_t e) { return std::string(cudaGetErrorName(e)) + ": " + cudaGetErrorString(e); }
+
+void check_cuda(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA ") + what + ": " + cuda_err(e));
+}
+
+int sm_count()
+{
+    int dev = 0, n = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n;
+}
+
+static int ceil_to(int x, int inc) { return ((x + inc - 1) / inc) * inc; }
+
+struct Geometry {
+    double prd[3], cen[3], cutneighmax, cutghost, binsize[3], bininv[3];
+    int mbin[3], n_col;
+    float rc2_tail;
+};
+
+static Geometry geometry(const Spec &s, int n)
+{
+    // neighbor.cpp:258-268, neighbor_meso.cu:771-853, neigh_list_meso.cu:78-90
+    Geometry g{};
+    double cutforce = 0;
+    for (int i = 0; i < s.ntype; ++i)
+        for (int j = 0; j < s.ntype; ++j) cutforce = std::max(cutforce, s.pair[i][j].cut);
+    g.cutneighmax = cutforce + s.skin;
+    g.cutghost = g.cutneighmax;
+    for (int d = 0; d < 3; ++d) {
+        g.prd[d] = s.hi[d] - s.lo[d];
+        g.cen[d] = 0.5 * (s.hi[d] + s.lo[d]);
+    }
+    const double vol = g.prd[0] * g.prd[1] * g.prd[2];
+    const double dens = s.rho_est > 0 ? s.rho_est : n / vol;
+    double e = dens * (4.0 / 3.0 * 3.142 * std::pow(g.cutneighmax, 3.0));
+    e *= 4.0;
+    e = std::max(e, 32.0);
+    g.n_col = ceil_to((int)e, 32);
+    const double inv_opt = 1.0 / g.cutneighmax;
+    for (int d = 0; d < 3; ++d) {
+        const int nb = std::max((int)(g.prd[d] * inv_opt), 1);
+        g.mbin[d] = nb + 2;
+        g.binsize[d] = g.prd[d] / nb;
+        g.bininv[d] = 1.0 / g.binsize[d];
+    }
+    g.rc2_tail = (float)std::pow(g.cutneighmax, 2.0);
+    return g;
+}
+
+static long long ghost_estimate(const Spec &s, const Geometry &g, int n)
+{
+    double f = 1.0;
+    for (int d = 0; d < 3; ++d) f *= 1.0 + 2.0 * g.cutghost / g.prd[d];
+    const double est = (f - 1.0) * n;
+    return (long long)(est * 1.5 * s.ghost_factor) + 4096;
+}
+
+size_t Box::estimate_bytes(const Spec &spec, int n)
+{
+    const Geometry g = geometry(spec, n);
+    const long long nbin = (long long)g.mbin[0] * g.mbin[1] * g.mbin[2];
+    const long long gc = ghost_estimate(spec, g, n);
+    const long long nrow = ceil_to(n, 32);
+    size_t b = 0;
+    b += (size_t)n * (2 * 6 * 8 + 3 * 8 + 2 * 16 + 6 * 4 + 2 * 4 + 3 * 4 + 4);  // x,v,xh,f,tag/type/mask,phi,cls,sub,perm,count
+    b += (size_t)(n + gc) * (16 + 16 + 4 + 4 + 4 + 16 + 4);                      // pos, vel, rho, bin_of, bin_order, bpos, gfirst
+    b += (size_t)gc * 8;
+    b += (size_t)nrow * g.n_col * 4;
+    b += (size_t)nbin * (4 + 3 * 4) * 3;
+    b += (size_t)((n + kUnit - 1) / kUnit) * kPartialStride * 8;
+    return b + (1u << 20);
+}
+
+template <class T> T *Box::alloc(size_t count)
+{
+    void *p = nullptr;
+    const size_t bytes_ = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&p, bytes_);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw std::runtime_error("OOM: cudaMalloc of " + std::to_string(bytes_) + " bytes failed");
+    }
+    check_cuda(cudaMemset(p, 0, bytes_), "memset");
+    allocs_.push_back(p);
+    bytes += bytes_;
+    return (T *)p;
+}
+
+Box::Box(const Spec &s, const Particles &p, int sms) : spec(s)
+{
+    (void)sms;
+    n = (int)p.size();
+    if (n <= 0) throw std::runtime_error("ARG: box has no particles");
+    if (s.ntype < 1 || s.ntype > kMaxTypes) throw std::runtime_error("ARG: 1..8 atom types supported");
+    for (int a = 0; a < s.ntype; ++a)
+        for (int b = 0; b < s.ntype; ++b)
+            if (!s.pair[a][b].set) throw std::runtime_error("PARSE: All pair coeffs are not set");
+    const Geometry g = geometry(s, n);
+    for (int d = 0; d < 3; ++d)
+        if (g.mbin[d] - 2 < 3)
+            throw std::runtime_error("ARG: box edge shorter than 3 x (cutoff + skin) is not supported");
+    std::memset(&desc, 0, sizeof(desc));
+    BoxDesc &B = desc;
+    for (int d = 0; d < 3; ++d) {
+        B.lo[d] = s.lo[d];
+        B.hi[d] = s.hi[d];
+        B.prd[d] = g.prd[d];
+        B.cen[d] = g.cen[d];
+        B.binsize[d] = g.binsize[d];
+        B.bininv[d] = g.bininv[d];
+        B.coord_inv[d] = 16 * g.bininv[d];
+        B.mbin[d] = g.mbin[d];
+    }
+    B.cutghost = g.cutghost;
+    B.triggersq = 0.25 * s.skin * s.skin;
+    B.rc2_tail = g.rc2_tail;
+    nbin = B.nbin = g.mbin[0] * g.mbin[1] * g.mbin[2];
+    B.nlocal = n;
+    B.nrow = ceil_to(n, 32);
+    B.ghost_cap = (int)std::min<long long>(ghost_estimate(s, g, n), 8LL * n + 4096);
+    B.n_col = g.n_col;
+    B.every = std::max(1, s.every);
+    B.delay = s.delay;
+    B.check = s.check;
+    B.style = s.style;
+    B.ntype = s.ntype;
+    B.exact_rng = s.exact_rng;
+    for (int a = 0; a < s.ntype; ++a)
+        for (int b = 0; b < s.ntype; ++b) {
+            const PairParam &q = s.pair[a][b];
+            PairCoeff &c = B.coeff[a * s.ntype + b];
+            c.cut = (float)q.cut;
+            c.cutsq = (float)(q.cut * q.cut);
+            c.inv_cut = (float)(1.0 / q.cut);
+            c.cut_r = (float)q.cut_r;
+            c.inv_cut_r = q.cut_r > 0 ? (float)(1.0 / q.cut_r) : 0.f;
+            c.A = (float)q.A;
+            c.B = (float)q.B;
+            c.gamma = (float)q.gamma;
+            // mdpd: sigma = sqrt(2 kB T gamma) (pair_mdpd_meso.cu:387); dpd: given
+            c.sigma = (float)(s.style == 0 ? std::sqrt(2.0 * s.kT * q.gamma) : q.sigma);
+            c.expw = (float)q.expw;
+            c.e_cut = (float)(0.5 * q.A * q.cut);
+            c.e_cut_r = (float)(0.5 * q.B * q.cut_r);
+        }
+    const double dtf = 0.5 * s.dt;  // ftm2v = 1 (units lj)
+    for (int t = 0; t < kMaxTypes; ++t) {
+        B.mass[t] = s.mass[t];
+        B.dtfm[t] = dtf * rcp_newton(s.mass[t]);
+    }
+    B.dtv = s.dt;
+    B.dtf = dtf;
+    B.dt_inv_sqrt = (float)(1.0 / std::sqrt(s.dt));
+    B.seed = s.seed;
+    B.nve_bit = s.nve_bit;
+    B.rho_bit = s.rho_bit;
+    B.cut_rho = (float)s.cut_rho;
+    B.rho_factor = (float)(15.0 / (2.0 * M_PI * std::pow(s.cut_rho, 5.0)));
+    B.body_bit = s.body_bit;
+    for (int d = 0; d < 3; ++d) B.body[d] = (float)s.body[d];
+    B.arb_bc = s.arb_bc;
+    B.mobile_bit = s.mobile_bit;
+    B.wall_bit = s.wall_bit;
+    B.wall_fix = s.wall_fix;
+    B.cut_phi = (float)s.cut_phi;
+    if (s.wall_fix) {
+        const double rc7 = std::pow(s.cut_phi, 7.0);
+        B.phi_factor = (float)(105.0 / (16.0 * M_PI * s.rho_wall * rc7));
+        B.dw_factor = (float)(-315.0 / (4.0 * M_PI * s.rho_wall * rc7));
+        B.phi_c = (float)s.phi_c;
+    }
+
+    const int na = n + B.ghost_cap;
+    for (int c = 0; c < 2; ++c) {
+        for (int d = 0; d < 3; ++d) {
+            B.x[c][d] = alloc<double>(n);
+            B.v[c][d] = alloc<double>(n);
+        }
+        B.f[c] = alloc<float4>(n);
+        B.tag[c] = alloc<int>(n);
+        B.type[c] = alloc<int>(n);
+        B.mask[c] = alloc<int>(n);
+        B.phi[c] = alloc<float>(n);
+    }
+    for (int d = 0; d < 3; ++d) B.xh[d] = alloc<double>(n);
+    B.pos = alloc<float4>(na);
+    B.vel = alloc<float4>(na);
+    B.rho = alloc<float>(na);
+    B.gsrc = alloc<int>(B.ghost_cap);
+    B.gimg = alloc<int>(B.ghost_cap);
+    B.gfirst = alloc<int>(n + 1);
+    B.count = alloc<int>(B.nrow);
+    B.table = alloc<int>((size_t)B.nrow * B.n_col);
+    B.bin_rank = alloc<int>(nbin);
+    B.cls_count = alloc<int>(2 * (size_t)nbin + 1);
+    B.cls_start = alloc<int>(2 * (size_t)nbin + 1);
+    B.cls_cursor = alloc<int>(2 * (size_t)nbin + 1);
+    B.cls_of = alloc<int>(n);
+    B.sub_of = alloc<int>(n);
+    B.perm = alloc<int>(n);
+    B.bin_of = alloc<int>(na);
+    B.bin_count = alloc<int>(nbin + 1);
+    B.bin_start = alloc<int>(nbin + 1);
+    B.bin_cursor = alloc<int>(nbin + 1);
+    B.bin_order = alloc<int>(na);
+    B.bpos = alloc<float4>(na);
+    const int nchunk = std::max({2 * nbin, n + 1, nbin}) / kScanChunk + 2;
+    B.scan_part = alloc<int>(nchunk);
+    B.partial = alloc<double>((size_t)((n + kUnit - 1) / kUnit) * kPartialStride);
+    d_state = alloc<BoxState>(1);
+    B.st = d_state;
+
+    // Morton rank of every bin: reorder buckets are visited in Morton order of their bin
+    {
+        std::vector<std::pair<uint64_t, int>> codes(nbin);
+        for (int z = 0, b = 0; z < g.mbin[2]; ++z)
+            for (int y = 0; y < g.mbin[1]; ++y)
+                for (int x = 0; x < g.mbin[0]; ++x, ++b) codes[b] = {morton3(x, y, z), b};
+        std::sort(codes.begin(), codes.end());
+        std::vector<int> rank(nbin);
+        for (int r = 0; r < nbin; ++r) rank[codes[r].second] = r;
+        check_cuda(cudaMemcpy(B.bin_rank, rank.data(), sizeof(int) * nbin, cudaMemcpyHostToDevice), "upload");
+    }
+    // initial state into buffer 0, component-separated
+    {
+        std::vector<double> col(n);
+        for (int d = 0; d < 3; ++d) {
+            for (int i = 0; i < n; ++i) col[i] = p.x[3 * i + d];
+            check_cuda(cudaMemcpy(B.x[0][d], col.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "upload");
+            check_cuda(cudaMemcpy(B.xh[d], col.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "upload");
+            for (int i = 0; i < n; ++i) col[i] = p.v[3 * i + d];
+            check_cuda(cudaMemcpy(B.v[0][d], col.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "upload");
+        }
+        check_cuda(cudaMemcpy(B.tag[0], p.tag.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
+        check_cuda(cudaMemcpy(B.type[0], p.type.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
+        check_cuda(cudaMemcpy(B.mask[0], p.mask.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
+        for (int i = 0; i < n; ++i)
+            if (p.mask[i] & s.nve_bit) ++n_group;
+    }
+}
+
+Box::~Box()
+{
+    for (void *p : allocs_) cudaFree(p);
+}
+
+BoxState Box::state() const
+{
+    BoxState st;
+    check_cuda(cudaMemcpy(&st, d_state, sizeof(st), cudaMemcpyDeviceToHost), "download state");
+    return st;
+}
+
+void Box::download_state(double *x, double *v, double *f, int32_t *tag, int32_t *type, int32_t *mask) const
+{
+    const BoxState st = state();
+    const int c = st.cur;
+    std::vector<double> col(n);
+    for (int d = 0; d < 3; ++d) {
+        if (x) {
+            check_cuda(cudaMemcpy(col.data(), desc.x[c][d], sizeof(double) * n, cudaMemcpyDeviceToHost), "download");
+            for (int i = 0; i < n; ++i) x[3 * i + d] = col[i];
+        }
+        if (v) {
+            check_cuda(cudaMemcpy(col.data(), desc.v[c][d], sizeof(double) * n, cudaMemcpyDeviceToHost), "download");
+            for (int i = 0; i < n; ++i) v[3 * i + d] = col[i];
+        }
+    }
+    if (f) {
+        std::vector<float4> ff(n);
+        check_cuda(cudaMemcpy(ff.data(), desc.f[c], sizeof(float4) * n, cudaMemcpyDeviceToHost), "download");
+        for (int i = 0; i < n; ++i) {
+            f[3 * i] = ff[i].x;
+            f[3 * i + 1] = ff[i].y;
+            f[3 * i + 2] = ff[i].z;
+        }
+    }
+    if (tag) check_cuda(cudaMemcpy(tag, desc.tag[c], sizeof(int) * n, cudaMemcpyDeviceToHost), "download");
+    if (type) check_cuda(cudaMemcpy(type, desc.type[c], sizeof(int) * n, cudaMemcpyDeviceToHost), "download");
+    if (mask) check_cuda(cudaMemcpy(mask, desc.mask[c], sizeof(int) * n, cudaMemcpyDeviceToHost), "download");
+}
+
+void Box::upload_xv(const double *x, const double *v)
+{
+    // x, v given in tag order (tag t at row t-1); scattered to the internal order
+    const BoxState st = state();
+    const int c = st.cur;
+    std::vector<int32_t> tag(n);
+    check_cuda(cudaMemcpy(tag.data(), desc.tag[c], sizeof(int) * n, cudaMemcpyDeviceToHost), "download");
+    std::vector<double> col(n);
+    for (int d = 0; d < 3; ++d) {
+        if (x) {
+            for (int i = 0; i < n; ++i) col[i] = x[3 * (tag[i] - 1) + d];
+            check_cuda(cudaMemcpy(desc.x[c][d], col.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "upload");
+        }
+        if (v) {
+            for (int i = 0; i < n; ++i) col[i] = v[3 * (tag[i] - 1) + d];
+            check_cuda(cudaMemcpy(desc.v[c][d], col.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "upload");
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+
+Batch::Batch(std::vector<Box *> boxes, const StepConfig &c) : cfg(c), boxes_(std::move(boxes))
+{
+    if (boxes_.empty()) throw std::runtime_error("ARG: empty batch");
+    check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+    const int nb = (int)boxes_.size();
+    check_cuda(cudaMalloc(&d_boxes, sizeof(BoxDesc) * nb), "boxes");
+    std::vector<BoxDesc> h(nb);
+    for (int b = 0; b < nb; ++b) h[b] = boxes_[b]->desc;
+    check_cuda(cudaMemcpy(d_boxes, h.data(), sizeof(BoxDesc) * nb, cudaMemcpyHostToDevice), "boxes");
+    check_cuda(cudaMalloc(&d_done, sizeof(int) * 4), "done");
+    check_cuda(cudaMemset(d_done, 0, sizeof(int) * 4), "done");
+    check_cuda(cudaMalloc(&d_thermo, sizeof(double) * kPartialStride * nb), "thermo");
+    build_units();
+    capture(0);
+    capture(1);
+}
+
+Batch::~Batch()
+{
+    for (int k = 0; k < 2; ++k) {
+        if (graph_[k]) cudaGraphExecDestroy(graph_[k]);
+        if (graph_src_[k]) cudaGraphDestroy(graph_src_[k]);
+    }
+    for (Unit *u : unit_allocs_) cudaFree(u);
+    cudaFree(d_boxes);
+    cudaFree(d_done);
+    cudaFree(d_thermo);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Batch::build_units()
+{
+    std::vector<Unit> loc, all, cls, bins, scls, sgh, sbin;
+    for (int b = 0; b < (int)boxes_.size(); ++b) {
+        const BoxDesc &B = boxes_[b]->desc;
+        auto chunk = [&](std::vector<Unit> &v, int n, int step) {
+            for (int s = 0; s < n; s += step) v.push_back({b, s, std::min(n, s + step)});
+        };
+        chunk(loc, B.nlocal, kUnit);
+        chunk(all, B.nlocal + B.ghost_cap, kUnit);
+        chunk(cls, 2 * B.nbin, 256);
+        chunk(bins, B.nbin, 256);
+        chunk(scls, 2 * B.nbin, kScanChunk);
+        chunk(sgh, B.nlocal + 1, kScanChunk);
+        chunk(sbin, B.nbin, kScanChunk);
+    }
+    auto up = [&](const std::vector<Unit> &v) {
+        Unit *d = nullptr;
+        check_cuda(cudaMalloc(&d, sizeof(Unit) * std::max<size_t>(v.size(), 1)), "units");
+        check_cuda(cudaMemcpy(d, v.data(), sizeof(Unit) * v.size(), cudaMemcpyHostToDevice), "units");
+        unit_allocs_.push_back(d);
+        return UnitList{d, (int)v.size()};
+    };
+    units.local = up(loc);
+    units.all = up(all);
+    units.cls = up(cls);
+    units.bins = up(bins);
+    units.scan_cls = up(scls);
+    units.scan_ghost = up(sgh);
+    units.scan_bin = up(sbin);
+    units.nbox = (int)boxes_.size();
+}
+
+void Batch::capture(int ev)
+{
+    cudaGraph_t g;
+    check_cuda(cudaGraphCreate(&g, 0), "graph create");
+    cudaGraphConditionalHandle h;
+    check_cuda(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault), "conditional handle");
+    check_cuda(cudaStreamBeginCaptureToGraph(stream_, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+               "capture");
+    launch_integrate(stream_, d_boxes, units, cfg, d_done, h, 1);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    check_cuda(cudaStreamGetCaptureInfo(stream_, &cs, nullptr, &cg, &deps, &nd), "capture info");
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.size = 1;
+    cudaGraphNode_t cn;
+    check_cuda(cudaGraphAddNode(&cn, cg, deps, nd, &p), "conditional node");
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    check_cuda(cudaStreamUpdateCaptureDependencies(stream_, &cn, 1, cudaStreamSetCaptureDependencies), "deps");
+    cudaStream_t s2;
+    check_cuda(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking), "stream");
+    check_cuda(cudaStreamBeginCaptureToGraph(s2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+               "capture body");
+    launch_rebuild(s2, d_boxes, units, cfg, d_done);
+    cudaGraph_t tmp;
+    check_cuda(cudaStreamEndCapture(s2, &tmp), "end body");
+    cudaStreamDestroy(s2);
+    if (cfg.style == 0) launch_density(stream_, d_boxes, units, cfg);
+    launch_force(stream_, d_boxes, units, cfg, ev, 1);
+    if (ev) launch_thermo(stream_, d_boxes, units, d_thermo, d_done + 2);
+    check_cuda(cudaStreamEndCapture(stream_, &tmp), "end capture");
+    check_cuda(cudaGraphInstantiate(&graph_[ev], g, 0), "instantiate");
+    graph_src_[ev] = g;
+}
+
+void Batch::setup()
+{
+    launch_force_rebuild_flag(stream_, d_boxes, units.nbox, 1);
+    launch_rebuild(stream_, d_boxes, units, cfg, d_done);
+    if (cfg.style == 0) launch_density(stream_, d_boxes, units, cfg);
+    launch_force(stream_, d_boxes, units, cfg, 1, 0);
+    launch_force_rebuild_flag(stream_, d_boxes, units.nbox, 0);
+    check_cuda(cudaGetLastError(), "setup launch");
+    check_cuda(cudaStreamSynchronize(stream_), "setup");
+}
+
+__global__ void k_set_rebuild(BoxDesc *boxes, const int *which, int nwhich, int nbox)
+{
+    for (int b = threadIdx.x; b < nbox; b += blockDim.x) boxes[b].st->rebuild = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < nwhich; k += blockDim.x) {
+        boxes[which[k]].st->rebuild = 1;
+        boxes[which[k]].st->ago = 0;
+    }
+}
+
+void Batch::setup_boxes(const std::vector<int> &which)
+{
+    if (which.empty()) return;
+    int *d = nullptr;
+    check_cuda(cudaMallocAsync(&d, sizeof(int) * which.size(), stream_), "setup boxes");
+    check_cuda(cudaMemcpyAsync(d, which.data(), sizeof(int) * which.size(), cudaMemcpyHostToDevice, stream_),
+               "setup boxes");
+    k_set_rebuild<<<1, 256, 0, stream_>>>(d_boxes, d, (int)which.size(), units.nbox);
+    launch_rebuild(stream_, d_boxes, units, cfg, d_done);
+    if (cfg.style == 0) launch_density(stream_, d_boxes, units, cfg);
+    launch_force(stream_, d_boxes, units, cfg, 1, 0);
+    launch_force_rebuild_flag(stream_, d_boxes, units.nbox, 0);
+    check_cuda(cudaFreeAsync(d, stream_), "setup boxes");
+    check_cuda(cudaGetLastError(), "setup launch");
+    check_cuda(cudaStreamSynchronize(stream_), "setup");
+}
+
+void Batch::reconfigure(const StepConfig &c)
+{
+    check_cuda(cudaStreamSynchronize(stream_), "reconfigure");
+    for (int k = 0; k < 2; ++k) {
+        if (graph_[k]) cudaGraphExecDestroy(graph_[k]);
+        if (graph_src_[k]) cudaGraphDestroy(graph_src_[k]);
+        graph_[k] = nullptr;
+        graph_src_[k] = nullptr;
+    }
+    cfg = c;
+    capture(0);
+    capture(1);
+}
+
+void Batch::run(long long nsteps, bool sync)
+{
+    for (long long k = 0; k < nsteps; ++k) check_cuda(cudaGraphLaunch(graph_[0], stream_), "graph launch");
+    if (sync) check_cuda(cudaStreamSynchronize(stream_), "run");
+}
+
+void Batch::step_ev() { check_cuda(cudaGraphLaunch(graph_[1], stream_), "graph launch"); }
+
+long long Batch::rebuild_steps()
+{
+    int h[4];
+    check_cuda(cudaMemcpy(h, d_done, sizeof(h), cudaMemcpyDeviceToHost), "counters");
+    return h[3];
+}
+
+void Batch::profile(long long nsteps, double out[5])
+{
+    cudaEvent_t ev[5];
+    for (auto &e : ev) check_cuda(cudaEventCreate(&e), "event");
+    double acc[4] = {0, 0, 0, 0};
+    const long long r0 = rebuild_steps();
+    for (long long k = 0; k < nsteps; ++k) {
+        cudaEventRecord(ev[0], stream_);
+        launch_integrate(stream_, d_boxes, units, cfg, d_done, cudaGraphConditionalHandle{}, 0);
+        cudaEventRecord(ev[1], stream_);
+        launch_rebuild(stream_, d_boxes, units, cfg, d_done);  // kernels skip boxes not rebuilding
+        cudaEventRecord(ev[2], stream_);
+        if (cfg.style == 0) launch_density(stream_, d_boxes, units, cfg);
+        cudaEventRecord(ev[3], stream_);
+        launch_force(stream_, d_boxes, units, cfg, 0, 1);
+        cudaEventRecord(ev[4], stream_);
+        check_cuda(cudaEventSynchronize(ev[4]), "profile");
+        for (int q = 0; q < 4; ++q) {
+            float t = 0;
+            cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+            acc[q] += t;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    for (int q = 0; q < 4; ++q) out[q] = acc[q] / (double)nsteps;
+    out[4] = (double)(rebuild_steps() - r0);
+}
+
+void Batch::thermo(std::vector<Thermo> &out)
+{
+    launch_thermo(stream_, d_boxes, units, d_thermo, d_done + 2);
+    check_cuda(cudaGetLastError(), "thermo launch");
+    const int nb = (int)boxes_.size();
+    std::vector<double> h((size_t)nb * kPartialStride);
+    check_cuda(cudaMemcpyAsync(h.data(), d_thermo, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream_),
+               "thermo download");
+    check_cuda(cudaStreamSynchronize(stream_), "thermo");
+    out.resize(nb);
+    for (int b = 0; b < nb; ++b) {
+        const Box &bx = *boxes_[b];
+        const BoxState st = bx.state();
+        Thermo &t = out[b];
+        const double *q = &h[(size_t)b * kPartialStride];
+        t.step = st.step;
+        t.nbuild = st.nbuild;
+        t.status = st.status;
+        t.ke_all = q[0];
+        for (int k = 0; k < 6; ++k) t.virial[k] = q[1 + k];
+        t.pe = q[7];
+        t.mom[0] = q[8], t.mom[1] = q[9], t.mom[2] = q[10];
+        t.ke_group = q[11];
+        t.n = bx.n;
+        t.n_group = bx.n_group;
+        // compute temp (all atoms, dof = 3N - 3) and pressure (compute_pressure_meso.cu:121-150)
+        const double dof = 3.0 * t.n - 3.0;
+        t.temp = dof > 0 ? t.ke_all / dof : 0.0;
+        const double vol = bx.desc.prd[0] * bx.desc.prd[1] * bx.desc.prd[2];
+        t.press = (dof * t.temp + t.virial[0] + t.virial[1] + t.virial[2]) / 3.0 / vol;
+    }
+}
+
+int Batch::status(std::string &msg)
+{
+    int all = 0;
+    for (size_t b = 0; b < boxes_.size(); ++b) {
+        const BoxState st = boxes_[b]->state();
+        if (st.status) {
+            all |= st.status;
+            msg += "box " + std::to_string(b) + ": status " + std::to_string(st.status) + "; ";
+        }
+    }
+    return all;
+}
+
+}  // namespace mdpd

@@ -1,0 +1,128 @@
+// Host runtime of the B200 DPD/mDPD timestep path: device-resident boxes, batches of
+// boxes stepped by one captured CUDA graph per step, thermo reductions.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+namespace mdpd {
+
+// physics + geometry of one box, in reference units (LAMMPS lj)
+struct PairParam {
+    int set = 0;
+    double cut = 0, cut_r = 0, A = 0, B = 0, gamma = 0, sigma = 0, expw = 1;
+};
+
+struct Spec {
+    int style = 0;  // 0 mdpd/meso, 1 dpd/meso
+    int ntype = 1;
+    double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+    double skin = 0.3;
+    int every = 1, delay = 0, check = 1;
+    double dt = 0.01;
+    double kT = 1.0;       // mdpd: sigma = sqrt(2 kT gamma)
+    uint32_t seed = 1;
+    double rho_est = 0;    // atom_style mdpd/atomic/meso density estimate (0: nlocal/volume)
+    PairParam pair[kMaxTypes][kMaxTypes];
+    double mass[kMaxTypes] = {1, 1, 1, 1, 1, 1, 1, 1};
+    int nve_bit = 1;       // group bitmask of fix nve/meso
+    int rho_bit = 1;       // group bitmask of fix aboundary/rho/meso
+    double cut_rho = 0.75;
+    int body_bit = 0;
+    double body[3] = {0, 0, 0};
+    int arb_bc = 0, mobile_bit = 0, wall_bit = 0;  // pair_style ... fluid_group wall_group
+    int wall_fix = 0;                              // aboundary wall/mobile given
+    double cut_phi = 0, rho_wall = 0, phi_c = 0;
+    int exact_rng = 0;
+    double ghost_factor = 1.0;   // ghost capacity multiplier
+};
+
+struct Particles {
+    std::vector<double> x, v;        // 3 per particle
+    std::vector<int32_t> tag, type, mask;
+    size_t size() const { return tag.size(); }
+};
+
+struct Thermo {
+    long long step = 0, nbuild = 0;
+    double ke_all = 0, ke_group = 0, pe = 0, virial[6] = {0, 0, 0, 0, 0, 0}, mom[3] = {0, 0, 0};
+    double temp = 0, press = 0;
+    int n = 0, n_group = 0;
+    int status = 0;
+};
+
+class Box {
+public:
+    Box(const Spec &spec, const Particles &p, int sms);
+    ~Box();
+    Box(const Box &) = delete;
+    Box &operator=(const Box &) = delete;
+
+    BoxDesc desc;       // host copy of the device descriptor (pointers + parameters)
+    BoxState *d_state;  // device scalars
+    Spec spec;
+    int n = 0;
+    int nbin = 0;
+    size_t bytes = 0;   // device memory held
+    int n_group = 0;
+
+    static size_t estimate_bytes(const Spec &spec, int n);
+
+    // host views (synchronous)
+    BoxState state() const;
+    void download_state(double *x, double *v, double *f, int32_t *tag, int32_t *type,
+                        int32_t *mask) const;           // current internal order
+    void upload_xv(const double *x, const double *v);  // by tag, host order of tags 1..n
+
+private:
+    std::vector<void *> allocs_;
+    template <class T> T *alloc(size_t count);
+};
+
+// A set of boxes stepped together; one box is the plain single-box path.
+class Batch {
+public:
+    Batch(std::vector<Box *> boxes, const StepConfig &cfg);
+    ~Batch();
+    Batch(const Batch &) = delete;
+    Batch &operator=(const Batch &) = delete;
+
+    void setup();                          // forced rebuild, density, force (no kick), thermo partials
+    // setup of the listed boxes only: rebuild flags set for them alone; the density and force
+    // passes rerun for all boxes, which reproduces the same forces for the others
+    void setup_boxes(const std::vector<int> &which);
+    void reconfigure(const StepConfig &c);  // new pair-pass shapes: recapture the step graphs
+    void run(long long nsteps, bool sync = true);  // nsteps graph replays
+    void step_ev();                        // one step with energy/virial (thermo step)
+    // nsteps un-captured steps with CUDA events around each kernel group; per-step averages
+    // in ms: [integrate, rebuild (all steps), density, force], plus steps that rebuilt
+    void profile(long long nsteps, double out[5]);
+    long long rebuild_steps();             // steps whose rebuild body ran (device counter)
+    void thermo(std::vector<Thermo> &out); // reduce + download (synchronous)
+    int status(std::string &msg);          // OR of box status words
+    cudaStream_t stream() const { return stream_; }
+    const std::vector<Box *> &boxes() const { return boxes_; }
+    StepConfig cfg;
+    BatchUnits units;
+    BoxDesc *d_boxes = nullptr;
+
+private:
+    std::vector<Box *> boxes_;
+    cudaStream_t stream_ = nullptr;
+    int *d_done = nullptr;
+    double *d_thermo = nullptr;
+    std::vector<Unit *> unit_allocs_;
+    cudaGraphExec_t graph_[2] = {nullptr, nullptr};  // [ev]
+    cudaGraph_t graph_src_[2] = {nullptr, nullptr};
+    void build_units();
+    void capture(int ev);
+};
+
+std::string cuda_err(cudaError_t e);
+void check_cuda(cudaError_t e, const char *what);
+int sm_count();
+
+}  // namespace mdpd

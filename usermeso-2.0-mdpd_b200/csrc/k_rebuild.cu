@@ -1,0 +1,554 @@
+// Neighbour rebuild pipeline, run for the boxes whose rebuild flag is set:
+//
+//   key      wrap into the box (MesoDomain::pbc, domain_meso.cu:58-110); 2-level reorder
+//            key = border | Morton(bin) | Morton(16^3 sub-bin) (atom_meso.cu:271-311,346-387)
+//            split into a bucket class (border, Morton rank of the bin) and a 12-bit sub key
+//   sort     deterministic bucket sort: count -> scan -> scatter -> per-bucket sort by
+//            (sub key, original index).  Equals the reference's stable LSD radix sort of the
+//            full key (sort_meso.h:364-443), i.e. the same permutation.
+//   permute  gather every per-particle array into the other buffer, pack FP32 state,
+//            count ghost images of border particles, bin the locals
+//   ghosts   periodic images x + s*prd of every particle within cutghost of a face
+//            (MesoComm::borders, comm_meso.cu:42-193), binned with gpu_assign_bin_id's rule
+//            (neighbor_meso.cu:390-425)
+//   bins     the same bucket sort over locals+ghosts by bin, index order inside a bin
+//   list     warp per bin: 27-bin stencil candidates against up to 32 centres at a time,
+//            ballot insertion (atomic-free) straight into the locally transposed table
+//            (gpu_build_neighbor_list, neigh_build_meso.cu:17-127; layout neigh_list_meso.cu:143-147)
+#include "kernels.h"
+
+namespace mdpd {
+
+enum { kSelCls = 0, kSelGhost = 1, kSelBin = 2 };
+
+__device__ __forceinline__ bool rebuilding(const BoxDesc &B) { return B.st->rebuild != 0; }
+
+// ---------------------------------------------------------------------------
+// R1: wrap + reorder key
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kUnit) k_rb_key(const BoxDesc *__restrict__ boxes,
+                                                  const Unit *__restrict__ units, int nunits)
+{
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        if (!rebuilding(B)) continue;
+        const int i = U.begin + threadIdx.x;
+        if (i >= U.end) continue;
+        const int c = B.st->cur;
+        uint32_t bid[3], sub[3];
+        bool border = false;
+        for (int d = 0; d < 3; ++d) {
+            double x = B.x[c][d][i];
+            if (x < B.lo[d]) x += B.prd[d];
+            if (x >= B.hi[d]) {
+                x -= B.prd[d];
+                x = fmax(x, B.lo[d]);
+            }
+            if (!(x >= B.lo[d] && x < B.hi[d])) atomicOr(&B.st->status, kErrLost);
+            B.x[c][d][i] = x;
+            bid[d] = (uint32_t)clamp_bin(bin_coord(x, B.lo[d], B.bininv[d]), B.mbin[d]);
+            const double off = __fma_rn(-(double)(uint32_t)(bid[d] - 1u), B.binsize[d], x);
+            sub[d] = (uint32_t)clamp_bin((int)__dmul_rn(off, B.coord_inv[d]), 16);
+            border |= (x <= B.lo[d] + B.cutghost) || (x >= B.hi[d] - B.cutghost);
+        }
+        const int bin = (int)(bid[0] + B.mbin[0] * (bid[1] + bid[2] * B.mbin[1]));
+        const int cls = (border ? B.nbin : 0) + B.bin_rank[bin];
+        B.cls_of[i] = cls;
+        B.sub_of[i] = (int)morton3(sub[0], sub[1], sub[2]);
+        atomicAdd(&B.cls_count[cls], 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// scans: per-box exclusive scans of a count array, three kernels without inter-block waits
+// ---------------------------------------------------------------------------
+template <int SEL> __device__ __forceinline__ int *scan_in(const BoxDesc &B)
+{
+    return SEL == kSelCls ? B.cls_count : SEL == kSelGhost ? B.gfirst : B.bin_count;
+}
+template <int SEL> __device__ __forceinline__ int scan_len(const BoxDesc &B)
+{
+    return SEL == kSelCls ? 2 * B.nbin : SEL == kSelGhost ? B.nlocal + 1 : B.nbin;
+}
+
+template <int SEL>
+__global__ void __launch_bounds__(256) k_scan_reduce(const BoxDesc *__restrict__ boxes,
+                                                     const Unit *__restrict__ units, int nunits)
+{
+    __shared__ int s_w[8];
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        if (!rebuilding(B)) continue;
+        const int *in = scan_in<SEL>(B);
+        int a = 0;
+        for (int k = U.begin + threadIdx.x; k < U.end; k += 256) a += in[k];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if ((threadIdx.x & 31) == 0) s_w[threadIdx.x / 32] = a;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int w = 0; w < 8; ++w) t += s_w[w];
+            B.scan_part[U.begin / kScanChunk] = t;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ int block_exclusive_scan_256(int v, int *s_w, int &total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x / 32;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[w] = x;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int t = threadIdx.x < 8 ? s_w[threadIdx.x] : 0;
+        for (int o = 1; o < 8; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (threadIdx.x < 8) s_w[8 + threadIdx.x] = t;
+    }
+    __syncthreads();
+    total = s_w[15];
+    const int base = w > 0 ? s_w[8 + w - 1] : 0;
+    const int r = base + x - v;
+    __syncthreads();
+    return r;
+}
+
+template <int SEL>
+__global__ void __launch_bounds__(256) k_scan_top(const BoxDesc *__restrict__ boxes, int nbox)
+{
+    __shared__ int s_w[16];
+    const int b = blockIdx.x;
+    if (b >= nbox) return;
+    const BoxDesc &B = boxes[b];
+    if (!rebuilding(B)) return;
+    const int nch = (scan_len<SEL>(B) + kScanChunk - 1) / kScanChunk;
+    int carry = 0;
+    for (int base = 0; base < nch; base += 256) {
+        const int k = base + threadIdx.x;
+        const int v = k < nch ? B.scan_part[k] : 0;
+        int total;
+        const int ex = block_exclusive_scan_256(v, s_w, total);
+        if (k < nch) B.scan_part[k] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) B.scan_part[nch] = carry;
+}
+
+template <int SEL>
+__global__ void __launch_bounds__(256) k_scan_down(const BoxDesc *__restrict__ boxes,
+                                                   const Unit *__restrict__ units, int nunits)
+{
+    __shared__ int s_w[16];
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        if (!rebuilding(B)) continue;
+        int *in = scan_in<SEL>(B);
+        const int n = scan_len<SEL>(B);
+        int carry = B.scan_part[U.begin / kScanChunk];
+        // 8 items per thread, blocked
+        int v[8];
+        const int k0 = U.begin + threadIdx.x * 8;
+        int local = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            v[q] = (k0 + q < U.end) ? in[k0 + q] : 0;
+            local += v[q];
+        }
+        int total;
+        int ex = block_exclusive_scan_256(local, s_w, total) + carry;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int k = k0 + q;
+            if (k < U.end) {
+                if (SEL == kSelCls) {
+                    B.cls_start[k] = ex;
+                    B.cls_cursor[k] = ex;
+                } else if (SEL == kSelGhost) {
+                    in[k] = ex;
+                } else {
+                    B.bin_start[k] = ex;
+                    B.bin_cursor[k] = ex;
+                }
+            }
+            ex += v[q];
+        }
+        if (U.end == n && threadIdx.x == 255) {
+            // totals: ghost count / bin_start[nbin] / class sentinel
+            const int tot = ex;
+            if (SEL == kSelGhost) B.st->nghost = tot;
+            if (SEL == kSelBin) B.bin_start[n] = tot;
+            if (SEL == kSelCls) B.cls_start[n] = tot;
+        }
+    }
+}
+
+template <int SEL>
+static void scan(cudaStream_t s, BoxDesc *boxes, const UnitList &ul, int nbox, int sms)
+{
+    const int grid = ul.n < sms * 4 ? (ul.n > 0 ? ul.n : 1) : sms * 4;
+    k_scan_reduce<SEL><<<grid, 256, 0, s>>>(boxes, ul.d, ul.n);
+    k_scan_top<SEL><<<nbox, 256, 0, s>>>(boxes, nbox);
+    k_scan_down<SEL><<<grid, 256, 0, s>>>(boxes, ul.d, ul.n);
+}
+
+// ---------------------------------------------------------------------------
+// R3: scatter locals into their reorder buckets
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kUnit) k_rb_scatter_cls(const BoxDesc *__restrict__ boxes,
+                                                          const Unit *__restrict__ units, int nunits)
+{
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        if (!rebuilding(B)) continue;
+        const int i = U.begin + threadIdx.x;
+        if (i >= U.end) continue;
+        const int p = atomicAdd(&B.cls_cursor[B.cls_of[i]], 1);
+        B.perm[p] = i;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// R4 / R10: warp per bucket, order members by (sub key, index) or by index
+// ---------------------------------------------------------------------------
+template <int MODE>  // 0: reorder classes -> perm, 1: bins -> bin_order + bpos
+__global__ void __launch_bounds__(256) k_rb_bucket(const BoxDesc *__restrict__ boxes,
+                                                   const Unit *__restrict__ units, int nunits)
+{
+    __shared__ unsigned long long s_key[8][kClassMax];
+    const int lane = threadIdx.x & 31, w = threadIdx.x / 32;
+    unsigned long long *key = s_key[w];
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        if (!rebuilding(B)) continue;
+        int *cnt = MODE == 0 ? B.cls_count : B.bin_count;
+        const int *start = MODE == 0 ? B.cls_start : B.bin_start;
+        int *arr = MODE == 0 ? B.perm : B.bin_order;
+        for (int b = U.begin + w; b < U.end; b += 8) {
+            const int n = cnt[b];
+            if (n == 0) continue;
+            const int s = start[b];
+            __syncwarp();
+            if (n > kClassMax) {
+                if (lane == 0) {
+                    atomicOr(&B.st->status, kErrBucketOverflow);
+                    cnt[b] = 0;
+                }
+                continue;
+            }
+            for (int e = lane; e < n; e += 32) {
+                const int idx = arr[s + e];
+                key[e] = MODE == 0 ? (((unsigned long long)(uint32_t)B.sub_of[idx] << 32) | (uint32_t)idx)
+                                   : (unsigned long long)(uint32_t)idx;
+            }
+            __syncwarp();
+            for (int e = lane; e < n; e += 32) {
+                const unsigned long long k = key[e];
+                int rank = 0;
+                for (int q = 0; q < n; ++q) rank += key[q] < k;
+                const int idx = (int)(uint32_t)k;
+                arr[s + rank] = idx;
+                if (MODE == 1) B.bpos[s + rank] = B.pos[idx];
+            }
+            __syncwarp();
+            if (lane == 0) cnt[b] = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// R5: permute into the other buffer; pack; ghost-image counts; bin the locals
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int image_mask(const BoxDesc &B, double x, int d)
+{
+    // bit 0: image at +prd (x within cutghost of lo), bit 1: image at -prd
+    int m = 0;
+    if (x <= B.lo[d] + B.cutghost) m |= 1;
+    if (x >= B.hi[d] - B.cutghost) m |= 2;
+    return m;
+}
+
+__device__ __forceinline__ int bits_count(int m) { return 1 + (m & 1) + ((m >> 1) & 1); }
+
+template <int STYLE>
+__global__ void __launch_bounds__(kUnit) k_rb_permute(BoxDesc *__restrict__ boxes,
+                                                      const Unit *__restrict__ units, int nunits,
+                                                      int nbox, int *done)
+{
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        if (!rebuilding(B)) continue;
+        const int k = U.begin + threadIdx.x;
+        if (k >= U.end) continue;
+        const int c = B.st->cur, o = 1 - c;
+        const int old = B.perm[k];
+        double x[3], v[3];
+        for (int d = 0; d < 3; ++d) {
+            x[d] = B.x[c][d][old];
+            v[d] = B.v[c][d][old];
+            B.x[o][d][k] = x[d];
+            B.v[o][d][k] = v[d];
+            B.xh[d][k] = x[d];
+        }
+        B.f[o][k] = B.f[c][old];
+        const int tag = B.tag[c][old], type = B.type[c][old], mask = B.mask[c][old];
+        B.tag[o][k] = tag;
+        B.type[o][k] = type;
+        B.mask[o][k] = mask;
+        B.phi[o][k] = B.phi[c][old];
+        // packed state for the current step (the step counter was advanced by integrate)
+        const uint32_t sn = seed_now(B.seed, B.st->step);
+        const float fvx = (float)v[0], fvy = (float)v[1], fvz = (float)v[2];
+        B.pos[k] = make_float4((float)(x[0] - B.cen[0]), (float)(x[1] - B.cen[1]),
+                               (float)(x[2] - B.cen[2]), pack_w(B, type, mask));
+        const uint32_t sg = STYLE == 0 ? sig_mdpd(tag, sn) : sig_dpd(tag, fvx, fvy, fvz, sn);
+        B.vel[k] = make_float4(fvx, fvy, fvz, __uint_as_float(sg));
+        // ghost images of this particle
+        int nimg = 1;
+        for (int d = 0; d < 3; ++d) nimg *= bits_count(image_mask(B, x[d], d));
+        B.gfirst[k] = nimg - 1;
+        if (k == B.nlocal - 1) B.gfirst[B.nlocal] = 0;
+        // bin of the local
+        int bid[3];
+        for (int d = 0; d < 3; ++d) bid[d] = clamp_bin(bin_coord(x[d], B.lo[d], B.bininv[d]), B.mbin[d]);
+        const int bin = bid[0] + B.mbin[0] * (bid[1] + bid[2] * B.mbin[1]);
+        B.bin_of[k] = bin;
+        atomicAdd(&B.bin_count[bin], 1);
+    }
+    __shared__ bool s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(done, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        for (int b = threadIdx.x; b < nbox; b += blockDim.x) {
+            BoxState *S = boxes[b].st;
+            if (S->rebuild) {
+                S->cur = 1 - S->cur;
+                S->n_bulk = boxes[b].cls_start[boxes[b].nbin];
+            }
+        }
+        if (threadIdx.x == 0) *done = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// R7: ghost images of border particles + their bins
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kUnit) k_rb_ghosts(const BoxDesc *__restrict__ boxes,
+                                                     const Unit *__restrict__ units, int nunits)
+{
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        if (!rebuilding(B)) continue;
+        const int k = U.begin + threadIdx.x;
+        if (k >= U.end || k < B.st->n_bulk) continue;
+        const int c = B.st->cur;
+        const int g0 = B.gfirst[k], g1 = B.gfirst[k + 1];
+        if (g1 == g0) continue;
+        double x[3];
+        int m[3];
+        for (int d = 0; d < 3; ++d) {
+            x[d] = B.x[c][d][k];
+            m[d] = image_mask(B, x[d], d);
+        }
+        const float4 vk = B.vel[k];
+        const float w = B.pos[k].w;
+        int g = g0;
+        for (int sz = -1; sz <= 1; ++sz) {
+            if (sz == 1 && !(m[2] & 1)) continue;
+            if (sz == -1 && !(m[2] & 2)) continue;
+            for (int sy = -1; sy <= 1; ++sy) {
+                if (sy == 1 && !(m[1] & 1)) continue;
+                if (sy == -1 && !(m[1] & 2)) continue;
+                for (int sx = -1; sx <= 1; ++sx) {
+                    if (sx == 1 && !(m[0] & 1)) continue;
+                    if (sx == -1 && !(m[0] & 2)) continue;
+                    if (sx == 0 && sy == 0 && sz == 0) continue;
+                    if (g >= B.ghost_cap) {
+                        atomicOr(&B.st->status, kErrGhostOverflow);
+                        continue;
+                    }
+                    const double gx = x[0] + sx * B.prd[0];
+                    const double gy = x[1] + sy * B.prd[1];
+                    const double gz = x[2] + sz * B.prd[2];
+                    const int gi = B.nlocal + g;
+                    B.gsrc[g] = k;
+                    B.gimg[g] = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
+                    B.pos[gi] = make_float4((float)(gx - B.cen[0]), (float)(gy - B.cen[1]),
+                                            (float)(gz - B.cen[2]), w);
+                    B.vel[gi] = vk;
+                    const double gc[3] = {gx, gy, gz};
+                    int bid[3];
+                    for (int d = 0; d < 3; ++d) {
+                        const double v = gc[d];
+                        const int b = clamp_bin(bin_coord(v, B.lo[d], B.bininv[d]), B.mbin[d]);
+                        bid[d] = v >= B.lo[d] ? (v <= B.hi[d] ? b : B.mbin[d] - 1) : 0;
+                    }
+                    const int bin = bid[0] + B.mbin[0] * (bid[1] + bid[2] * B.mbin[1]);
+                    B.bin_of[gi] = bin;
+                    atomicAdd(&B.bin_count[bin], 1);
+                    ++g;
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// R9: scatter locals+ghosts into bins
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__restrict__ boxes,
+                                                           const Unit *__restrict__ units, int nunits)
+{
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        if (!rebuilding(B)) continue;
+        const int i = U.begin + threadIdx.x;
+        if (i >= U.end || i >= B.nlocal + min(B.st->nghost, B.ghost_cap)) continue;
+        const int p = atomicAdd(&B.bin_cursor[B.bin_of[i]], 1);
+        B.bin_order[p] = i;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// R11: neighbour list, warp per bin
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_rb_list(const BoxDesc *__restrict__ boxes,
+                                                 const Unit *__restrict__ units, int nunits,
+                                                 int nbox, int *done)
+{
+    __shared__ float s_x[8][32], s_y[8][32], s_z[8][32];
+    __shared__ int s_i[8][32], s_n[8][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x / 32;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        if (!rebuilding(B)) continue;
+        const float rc2 = B.rc2_tail;
+        const int ncol = B.n_col, nlocal = B.nlocal;
+        int local_max = 0;
+        for (int b = U.begin + w; b < U.end; b += 8) {
+            const int s = B.bin_start[b], e = B.bin_start[b + 1];
+            if (e == s || B.bin_order[s] >= nlocal) continue;  // no locals in this bin
+            const int bx = b % B.mbin[0], by = (b / B.mbin[0]) % B.mbin[1], bz = b / (B.mbin[0] * B.mbin[1]);
+            for (int cb = s; cb < e; cb += 32) {
+                // centre batch: members with index < nlocal (they come first)
+                const int pc = cb + lane;
+                int ci = pc < e ? B.bin_order[pc] : nlocal;
+                const bool is_c = ci < nlocal;
+                const unsigned cm = __ballot_sync(0xffffffffu, is_c);
+                if (cm == 0) break;
+                const int nc = __popc(cm);
+                if (is_c) {
+                    const float4 p = B.bpos[pc];
+                    s_x[w][lane] = p.x, s_y[w][lane] = p.y, s_z[w][lane] = p.z;
+                    s_i[w][lane] = ci;
+                    s_n[w][lane] = 0;
+                }
+                __syncwarp();
+                for (int dz = -1; dz <= 1; ++dz) {
+                    const int z = bz + dz;
+                    if (z < 0 || z >= B.mbin[2]) continue;
+                    for (int dy = -1; dy <= 1; ++dy) {
+                        const int y = by + dy;
+                        if (y < 0 || y >= B.mbin[1]) continue;
+                        for (int dx = -1; dx <= 1; ++dx) {
+                            const int x = bx + dx;
+                            if (x < 0 || x >= B.mbin[0]) continue;
+                            const int nb = x + B.mbin[0] * (y + z * B.mbin[1]);
+                            const int ps = B.bin_start[nb], pe = B.bin_start[nb + 1];
+                            for (int p0 = ps; p0 < pe; p0 += 32) {
+                                const int p = p0 + lane;
+                                const bool valid = p < pe;
+                                float4 pj = make_float4(1e30f, 1e30f, 1e30f, 0.f);
+                                int j = -1;
+                                if (valid) {
+                                    pj = B.bpos[p];
+                                    j = B.bin_order[p];
+                                }
+                                for (int q = 0; q < nc; ++q) {
+                                    const float ddx = s_x[w][q] - pj.x, ddy = s_y[w][q] - pj.y,
+                                                ddz = s_z[w][q] - pj.z;
+                                    const float r2 = dist2(ddx, ddy, ddz);
+                                    const int cq = s_i[w][q];
+                                    const bool hit = valid && r2 <= rc2 && j != cq;
+                                    const unsigned bal = __ballot_sync(0xffffffffu, hit);
+                                    if (bal) {
+                                        const int kq = s_n[w][q] + __popc(bal & lt);
+                                        if (hit && kq < ncol) B.table[list_addr(cq, kq, ncol)] = j;
+                                        __syncwarp();
+                                        if (lane == 0) s_n[w][q] += __popc(bal);
+                                        __syncwarp();
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+                if (is_c) {
+                    const int n = s_n[w][lane];
+                    B.count[ci] = n < ncol ? n : ncol;
+                    if (n > ncol) atomicOr(&B.st->status, kErrListOverflow);
+                    local_max = max(local_max, n);
+                }
+                __syncwarp();
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) local_max = max(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
+        if (lane == 0 && local_max > 0) atomicMax(&B.st->max_count, local_max);
+    }
+    __shared__ bool s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(done, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        for (int b = threadIdx.x; b < nbox; b += blockDim.x) {
+            BoxState *S = boxes[b].st;
+            if (S->rebuild) S->nbuild += 1;
+        }
+        if (threadIdx.x == 0) *done = 0;
+    }
+}
+
+void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int *done)
+{
+    const int sms = c.sms;
+    auto g = [&](int n, int per_sm) { return n < sms * per_sm ? (n > 0 ? n : 1) : sms * per_sm; };
+    k_rb_key<<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
+    scan<kSelCls>(s, boxes, u.scan_cls, u.nbox, sms);
+    k_rb_scatter_cls<<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
+    k_rb_bucket<0><<<g(u.cls.n, 4), 256, 0, s>>>(boxes, u.cls.d, u.cls.n);
+    if (c.style == 0)
+        k_rb_permute<0><<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done);
+    else
+        k_rb_permute<1><<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done);
+    scan<kSelGhost>(s, boxes, u.scan_ghost, u.nbox, sms);
+    k_rb_ghosts<<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
+    scan<kSelBin>(s, boxes, u.scan_bin, u.nbox, sms);
+    k_rb_scatter_bins<<<g(u.all.n, 8), kUnit, 0, s>>>(boxes, u.all.d, u.all.n);
+    k_rb_bucket<1><<<g(u.bins.n, 4), 256, 0, s>>>(boxes, u.bins.d, u.bins.n);
+    k_rb_list<<<g(u.bins.n, 4), 256, 0, s>>>(boxes, u.bins.d, u.bins.n, u.nbox, done + 1);
+}
+
+}  // namespace mdpd

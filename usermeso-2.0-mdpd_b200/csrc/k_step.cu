@@ -1,0 +1,563 @@
+// Per-step kernels: fused velocity-Verlet integrate + FP32 pack + ghost refresh,
+// the mDPD density pass, the mDPD/DPD force pass (with the final half-kick fused into
+// its epilogue) and the deterministic FP64 thermo reductions.
+//
+// Reference semantics:
+//   integrate      fix_nve_meso.cu:62-95 and :157-178 (FP64 x,v; dtfm = dtf*rcp(m))
+//   pack           atom_vec_mdpd_atomic_meso.cu:140-175, atom_vec_meso.cu:142-168
+//   ghosts         periodic images x + s*prd of comm_meso.cu:42-193, built on the device
+//   wall           fix_aboundary_rho_meso.cu:220-287
+//   density        fix_aboundary_rho_meso.cu:119-165
+//   force (mdpd)   pair_mdpd_meso.cu:93-228
+//   force (dpd)    pair_dpd_meso.cu:91-205
+//   rebuild check  neighbor.cpp:1216-1231 (decide), :1244-1322 (check_distance)
+#include "kernels.h"
+
+#include <cstdio>
+
+namespace mdpd {
+
+__device__ __forceinline__ bool last_block(int *done)
+{
+    __shared__ bool s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(done, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    return s_last;
+}
+
+// ---------------------------------------------------------------------------
+// integrate: initial half-kick + drift (+ wall bounce-back), displacement check,
+// FP32 pack of locals and their ghost images.  The last block decides the rebuild
+// per box (LAMMPS Neighbor::decide) and sets the graph's conditional.
+// ---------------------------------------------------------------------------
+template <bool WALL, int STYLE>
+__global__ void __launch_bounds__(kUnit) k_integrate(BoxDesc *__restrict__ boxes,
+                                                     const Unit *__restrict__ units, int nunits,
+                                                     int nbox, int *done,
+                                                     cudaGraphConditionalHandle cond, int use_cond)
+{
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        const int c = B.st->cur;
+        const int i = U.begin + threadIdx.x;
+        bool moved = false;
+        if (i < U.end) {
+            const long long step = B.st->step + 1;
+            const int t = B.type[c][i], m = B.mask[c][i];
+            double x = B.x[c][0][i], y = B.x[c][1][i], z = B.x[c][2][i];
+            double vx = B.v[c][0][i], vy = B.v[c][1][i], vz = B.v[c][2][i];
+            if (m & B.nve_bit) {
+                const float4 f = B.f[c][i];
+                const double dtfm = B.dtfm[t - 1];
+                vx = __fma_rn(dtfm, (double)f.x, vx);
+                vy = __fma_rn(dtfm, (double)f.y, vy);
+                vz = __fma_rn(dtfm, (double)f.z, vz);
+                x = __fma_rn(B.dtv, vx, x);
+                y = __fma_rn(B.dtv, vy, y);
+                z = __fma_rn(B.dtv, vz, z);
+            }
+            if (WALL && B.wall_fix && (m & B.mobile_bit)) {
+                // wall volume fraction and normal from frozen wall neighbours (old list)
+                const float cx = (float)x, cy = (float)y, cz = (float)z;
+                double phi_i = 0.0;
+                float nx = 0.f, ny = 0.f, nz = 0.f;
+                const int n = B.count[i];
+                const float cp = B.cut_phi;
+                for (int k = 0; k < n; ++k) {
+                    const int j = B.table[list_addr(i, k, B.n_col)];
+                    const float4 pj = B.pos[j];
+                    if (!(pflags(pj) & 2)) continue;
+                    int s = j, code = 13;
+                    if (j >= B.nlocal) {
+                        s = B.gsrc[j - B.nlocal];
+                        code = B.gimg[j - B.nlocal];
+                    }
+                    const float jx = (float)(B.x[c][0][s] + (code % 3 - 1) * B.prd[0]);
+                    const float jy = (float)(B.x[c][1][s] + ((code / 3) % 3 - 1) * B.prd[1]);
+                    const float jz = (float)(B.x[c][2][s] + (code / 9 - 1) * B.prd[2]);
+                    const float dx = cx - jx, dy = cy - jy, dz = cz - jz;
+                    const float rsq = dist2(dx, dy, dz);
+                    if (rsq < cp * cp) {
+                        const float rinv = rsqrtf(rsq);
+                        const float r = fmaxf(rsq * rinv, 1e-10f);
+                        const float d = cp - r;
+                        phi_i += (double)((cp + 3.f * r) * d * d * d * B.phi_factor);
+                        const float w = r * d * d * B.dw_factor * rinv;
+                        nx -= w * dx;
+                        ny -= w * dy;
+                        nz -= w * dz;
+                    }
+                }
+                B.phi[c][i] = (float)phi_i;
+                if (phi_i > B.phi_c) {
+                    const float nn = rsqrtf(nx * nx + ny * ny + nz * nz);
+                    nx *= nn, ny *= nn, nz *= nn;
+                    const double dtfm = B.dtf / B.mass[t - 1];
+                    const double ox = x - vx * dtfm, oy = y - vy * dtfm, oz = z - vz * dtfm;
+                    const double tt = fmax(0.0, vx * nx + vy * ny + vz * nz);
+                    vx = -vx + 2.0 * tt * nx;
+                    vy = -vy + 2.0 * tt * ny;
+                    vz = -vz + 2.0 * tt * nz;
+                    x = ox + B.dtv * vx;
+                    y = oy + B.dtv * vy;
+                    z = oz + B.dtv * vz;
+                }
+            }
+            B.v[c][0][i] = vx, B.v[c][1][i] = vy, B.v[c][2][i] = vz;
+            B.x[c][0][i] = x, B.x[c][1][i] = y, B.x[c][2][i] = z;
+            const double ddx = x - B.xh[0][i], ddy = y - B.xh[1][i], ddz = z - B.xh[2][i];
+            moved = ddx * ddx + ddy * ddy + ddz * ddz > B.triggersq;
+            // pack
+            const uint32_t sn = seed_now(B.seed, step);
+            const float w = pack_w(B, t, m);
+            const float4 p = make_float4((float)(x - B.cen[0]), (float)(y - B.cen[1]),
+                                         (float)(z - B.cen[2]), w);
+            const float fvx = (float)vx, fvy = (float)vy, fvz = (float)vz;
+            const int tag = B.tag[c][i];
+            const uint32_t sg = STYLE == 0 ? sig_mdpd(tag, sn) : sig_dpd(tag, fvx, fvy, fvz, sn);
+            const float4 vv = make_float4(fvx, fvy, fvz, __uint_as_float(sg));
+            B.pos[i] = p;
+            B.vel[i] = vv;
+            if (i >= B.st->n_bulk) {
+                const int g1 = min(B.gfirst[i + 1], B.ghost_cap);  // an overflowed build is reported, never written past
+                for (int g = B.gfirst[i]; g < g1; ++g) {
+                    const int code = B.gimg[g];
+                    B.pos[B.nlocal + g] =
+                        make_float4((float)(x + (code % 3 - 1) * B.prd[0] - B.cen[0]),
+                                    (float)(y + ((code / 3) % 3 - 1) * B.prd[1] - B.cen[1]),
+                                    (float)(z + (code / 9 - 1) * B.prd[2] - B.cen[2]), w);
+                    B.vel[B.nlocal + g] = vv;
+                }
+            }
+        }
+        if (__syncthreads_or(moved) && threadIdx.x == 0) atomicOr(&B.st->moved, 1);
+    }
+    if (last_block(done)) {
+        int any = 0;
+        for (int b = threadIdx.x; b < nbox; b += blockDim.x) {
+            BoxState *S = boxes[b].st;
+            const BoxDesc &B = boxes[b];
+            const int moved = atomicExch(&S->moved, 0);
+            const int ago = S->ago + 1;
+            int rb = 0;
+            if (ago >= B.delay && ago % B.every == 0) rb = B.check ? moved : 1;
+            S->rebuild = rb;
+            S->ago = rb ? 0 : ago;
+            S->step += 1;
+            any |= rb;
+        }
+        any = __syncthreads_or(any);
+        if (threadIdx.x == 0) {
+            *done = 0;
+            if (any) done[3] += 1;  // steps that ran the rebuild body
+            if (use_cond) cudaGraphSetConditional(cond, any ? 1u : 0u);
+        }
+    }
+}
+
+void launch_integrate(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c,
+                      int *done, cudaGraphConditionalHandle cond, int use_cond)
+{
+    int grid = u.local.n < c.sms * 8 ? u.local.n : c.sms * 8;
+    if (grid < 1) grid = 1;
+    if (c.wall) {
+        if (c.style == 0)
+            k_integrate<true, 0><<<grid, kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done, cond, use_cond);
+        else
+            k_integrate<true, 1><<<grid, kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done, cond, use_cond);
+    } else {
+        if (c.style == 0)
+            k_integrate<false, 0><<<grid, kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done, cond, use_cond);
+        else
+            k_integrate<false, 1><<<grid, kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done, cond, use_cond);
+    }
+}
+
+__global__ void k_force_rebuild_flag(BoxDesc *boxes, int nbox, int value)
+{
+    for (int b = threadIdx.x; b < nbox; b += blockDim.x) {
+        boxes[b].st->rebuild = value;
+        if (value) boxes[b].st->ago = 0;
+    }
+}
+
+void launch_force_rebuild_flag(cudaStream_t s, BoxDesc *boxes, int nbox, int value)
+{
+    k_force_rebuild_flag<<<1, 256, 0, s>>>(boxes, nbox, value);
+}
+
+// ---------------------------------------------------------------------------
+// density pass: rho_i = m_i * 15/(2 pi h^5) * sum_{r<h} (h - r)^2 over the list.
+// TPP threads per particle split the list and combine with shuffles.
+// ---------------------------------------------------------------------------
+template <int TPP>
+__global__ void __launch_bounds__(kUnit *TPP) k_density(const BoxDesc *__restrict__ boxes,
+                                                         const Unit *__restrict__ units, int nunits)
+{
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        const int i = U.begin + threadIdx.x / TPP;
+        const int t = threadIdx.x % TPP;
+        float acc = 0.f;
+        const bool live = i < U.end;
+        const int c = B.st->cur;
+        const bool in_group = live && (B.mask[c][i] & B.rho_bit);
+        if (in_group) {
+            const float4 pi = B.pos[i];
+            const float h = B.cut_rho, h2 = h * h;
+            const int n = B.count[i];
+            const int *row = B.table + (i & ~31) * B.n_col + (i & 31);
+            for (int k = t; k < n; k += TPP) {
+                const int j = __ldg(row + (k & 31) * B.n_col + (k & ~31));
+                const float4 pj = __ldg(&B.pos[j]);
+                const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                const float rsq = dist2(dx, dy, dz);
+                if (rsq < h2 && rsq >= 1e-20f) {
+                    const float d = h - sqrtf(rsq);
+                    acc = __fmaf_rn(d, d, acc);
+                }
+            }
+        }
+#pragma unroll
+        for (int o = TPP / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (in_group && t == 0) {
+            const float r = (float)(B.mass[ptype(B.pos[i])] * (double)B.rho_factor) * acc;
+            B.rho[i] = r;
+            if (i >= B.st->n_bulk) {
+                const int g1 = min(B.gfirst[i + 1], B.ghost_cap);
+                for (int g = B.gfirst[i]; g < g1; ++g) B.rho[B.nlocal + g] = r;
+            }
+        }
+    }
+}
+
+void launch_density(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c)
+{
+    const int grid = u.local.n < c.sms * 16 ? (u.local.n > 0 ? u.local.n : 1) : c.sms * 16;
+    switch (c.tpp_density) {
+    case 2: k_density<2><<<grid, kUnit * 2, 0, s>>>(boxes, u.local.d, u.local.n); break;
+    case 4: k_density<4><<<grid, kUnit * 4, 0, s>>>(boxes, u.local.d, u.local.n); break;
+    default: k_density<1><<<grid, kUnit, 0, s>>>(boxes, u.local.d, u.local.n); break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// force pass.  Per list entry: FP32 distance test against the type-pair cutoff; inside
+// it, the conservative + dissipative + random force with the pairwise gaussian of the
+// two signatures.  Epilogue (t==0): + body force, store f, final half-kick (FP64 v).
+// ---------------------------------------------------------------------------
+struct EvAcc {
+    float vxx, vyy, vzz, vxy, vxz, vyz, pe;
+};
+
+template <int TPP, int STYLE, bool EXACT, bool EV, bool WALLC>
+__global__ void __launch_bounds__(kUnit *TPP) k_force(const BoxDesc *__restrict__ boxes,
+                                                       const Unit *__restrict__ units, int nunits, int kick)
+{
+    __shared__ PairCoeff s_coeff[kMaxTypes * kMaxTypes];
+    __shared__ double s_red[kUnit * TPP / 32][7];
+    int cur_box = -1;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        if (U.box != cur_box) {
+            __syncthreads();
+            const int nc = B.ntype * B.ntype;
+            for (int q = threadIdx.x; q < nc; q += blockDim.x) s_coeff[q] = B.coeff[q];
+            cur_box = U.box;
+            __syncthreads();
+        }
+        const int ntype = B.ntype;
+        const int i = U.begin + threadIdx.x / TPP;
+        const int t = threadIdx.x % TPP;
+        const bool live = i < U.end;
+        float fx = 0.f, fy = 0.f, fz = 0.f;
+        EvAcc ev = {0, 0, 0, 0, 0, 0, 0};
+        float4 pi = make_float4(0, 0, 0, 0);
+        const int c = B.st->cur;
+        if (live) {
+            pi = B.pos[i];
+            const float4 vi = B.vel[i];
+            const uint32_t si = __float_as_uint(vi.w);
+            const int ti = ptype(pi);
+            const float rho_i = STYLE == 0 ? B.rho[i] : 0.f;
+            float wall_ratio = 1.f, wall_sqrt = 1.f;
+            const bool i_mobile = WALLC && (pflags(pi) & 1);
+            if (WALLC && i_mobile) {
+                // gamma/sigma scaling of (mobile, wall) pairs from phi_i (pair_mdpd_meso.cu:171-185);
+                // with h = h'*rcw the ratio depends on h' only
+                const float ph = fminf(B.phi[c][i], 0.5f);
+                const float hp = fmaxf(1.f - sqrtf(sqrtf(2.088f * ph * ph * ph + 1.478f * ph)), 0.025f);
+                const float q = 1.f - hp;
+                wall_ratio = 1.f + 0.187f * (1.f / hp - 1.f) - 0.093f * q * q * q;
+                wall_sqrt = sqrtf(wall_ratio);
+            }
+            const float dtis = B.dt_inv_sqrt;
+            const int n = B.count[i];
+            const int *row = B.table + (i & ~31) * B.n_col + (i & 31);
+            for (int k = t; k < n; k += TPP) {
+                const int j = __ldg(row + (k & 31) * B.n_col + (k & ~31));
+                const float4 pj = __ldg(&B.pos[j]);
+                const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                const float rsq = dist2(dx, dy, dz);
+                const PairCoeff &cf = s_coeff[ti * ntype + ptype(pj)];
+                if (rsq < cf.cutsq && rsq >= 1e-20f) {
+                    const float4 vj = __ldg(&B.vel[j]);
+                    const float rinv = rsqrtf(rsq);
+                    const float r = rsq * rinv;
+                    if (r < 1e-10f) continue;
+                    const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+                    const float dot = __fmaf_rn(dz, dvz, __fmaf_rn(dy, dvy, dx * dvx));
+                    const float wc = 1.f - r * cf.inv_cut;
+                    float gam = cf.gamma, sig = cf.sigma;
+                    float rn;
+                    if (EXACT)
+                        rn = (float)gaussian_exact(si, __float_as_uint(vj.w));
+                    else
+                        rn = gaussian_fast(si, __float_as_uint(vj.w));
+                    float fpair;
+                    if (STYLE == 0) {
+                        const float wcr = fmaxf(1.f - r * cf.inv_cut_r, 0.f);
+                        const float rho_j = __ldg(&B.rho[j]);
+                        if (WALLC && i_mobile && (pflags(pj) & 2)) {
+                            sig *= wall_sqrt;
+                            gam *= wall_ratio;
+                        }
+                        fpair = (cf.A * wc + cf.B * (rho_i + rho_j) * wcr) - gam * wc * wc * dot * rinv +
+                                sig * wc * rn * dtis;
+                        if (EV) ev.pe += cf.e_cut * wc * wc + cf.e_cut_r * (rho_i + rho_j) * wcr * wcr;
+                    } else {
+                        const float wr = cf.expw == 1.f ? wc : __powf(wc, cf.expw);
+                        fpair = cf.A * wc - gam * wr * wr * dot * rinv + sig * wr * rn * dtis;
+                        if (EV) ev.pe += cf.e_cut * wc * wc;
+                    }
+                    fpair *= rinv;
+                    fx = __fmaf_rn(dx, fpair, fx);
+                    fy = __fmaf_rn(dy, fpair, fy);
+                    fz = __fmaf_rn(dz, fpair, fz);
+                    if (EV) {
+                        ev.vxx += dx * dx * fpair;
+                        ev.vyy += dy * dy * fpair;
+                        ev.vzz += dz * dz * fpair;
+                        ev.vxy += dx * dy * fpair;
+                        ev.vxz += dx * dz * fpair;
+                        ev.vyz += dy * dz * fpair;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int o = TPP / 2; o > 0; o >>= 1) {
+            fx += __shfl_xor_sync(0xffffffffu, fx, o);
+            fy += __shfl_xor_sync(0xffffffffu, fy, o);
+            fz += __shfl_xor_sync(0xffffffffu, fz, o);
+            if (EV) {
+                ev.vxx += __shfl_xor_sync(0xffffffffu, ev.vxx, o);
+                ev.vyy += __shfl_xor_sync(0xffffffffu, ev.vyy, o);
+                ev.vzz += __shfl_xor_sync(0xffffffffu, ev.vzz, o);
+                ev.vxy += __shfl_xor_sync(0xffffffffu, ev.vxy, o);
+                ev.vxz += __shfl_xor_sync(0xffffffffu, ev.vxz, o);
+                ev.vyz += __shfl_xor_sync(0xffffffffu, ev.vyz, o);
+                ev.pe += __shfl_xor_sync(0xffffffffu, ev.pe, o);
+            }
+        }
+        if (live && t == 0) {
+            const int m = B.mask[c][i];
+            if (m & B.body_bit) {
+                fx += B.body[0];
+                fy += B.body[1];
+                fz += B.body[2];
+            }
+            if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&B.st->status, kErrNonFinite);
+            B.f[c][i] = make_float4(fx, fy, fz, 0.f);
+            if (kick && (m & B.nve_bit)) {
+                const double dtfm = B.dtfm[ptype(pi)];
+                B.v[c][0][i] = __fma_rn(dtfm, (double)fx, B.v[c][0][i]);
+                B.v[c][1][i] = __fma_rn(dtfm, (double)fy, B.v[c][1][i]);
+                B.v[c][2][i] = __fma_rn(dtfm, (double)fz, B.v[c][2][i]);
+            }
+        }
+        if (EV) {
+            // per-unit FP64 partials in a fixed order (deterministic)
+            double vals[7] = {0, 0, 0, 0, 0, 0, 0};
+            if (live && t == 0) {
+                vals[0] = 0.5 * ev.vxx, vals[1] = 0.5 * ev.vyy, vals[2] = 0.5 * ev.vzz;
+                vals[3] = 0.5 * ev.vxy, vals[4] = 0.5 * ev.vxz, vals[5] = 0.5 * ev.vyz;
+                vals[6] = 0.5 * ev.pe;
+            }
+#pragma unroll
+            for (int q = 0; q < 7; ++q)
+                for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_down_sync(0xffffffffu, vals[q], o);
+            const int w = threadIdx.x / 32;
+            if ((threadIdx.x & 31) == 0)
+                for (int q = 0; q < 7; ++q) s_red[w][q] = vals[q];
+            __syncthreads();
+            if (threadIdx.x < 7) {
+                double a = 0.0;
+                for (int ww = 0; ww < (int)(blockDim.x / 32); ++ww) a += s_red[ww][threadIdx.x];
+                B.partial[(size_t)(U.begin / kUnit) * kPartialStride + 1 + threadIdx.x] = a;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <int TPP, int STYLE, bool EXACT, bool EV>
+static void force_launch_wall(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, int grid, int wallc, int kick)
+{
+    if (wallc)
+        k_force<TPP, STYLE, EXACT, EV, true><<<grid, kUnit * TPP, 0, s>>>(boxes, u.local.d, u.local.n, kick);
+    else
+        k_force<TPP, STYLE, EXACT, EV, false><<<grid, kUnit * TPP, 0, s>>>(boxes, u.local.d, u.local.n, kick);
+}
+
+template <int TPP, int STYLE>
+static void force_launch_tpp(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, int grid,
+                             const StepConfig &c, int ev, int kick)
+{
+    if (c.exact_rng) {
+        if (ev) force_launch_wall<TPP, STYLE, true, true>(s, boxes, u, grid, c.wall_coupling, kick);
+        else force_launch_wall<TPP, STYLE, true, false>(s, boxes, u, grid, c.wall_coupling, kick);
+    } else {
+        if (ev) force_launch_wall<TPP, STYLE, false, true>(s, boxes, u, grid, c.wall_coupling, kick);
+        else force_launch_wall<TPP, STYLE, false, false>(s, boxes, u, grid, c.wall_coupling, kick);
+    }
+}
+
+template <int STYLE>
+static void force_launch_style(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, int grid,
+                               const StepConfig &c, int ev, int kick)
+{
+    switch (c.tpp_force) {
+    case 2: force_launch_tpp<2, STYLE>(s, boxes, u, grid, c, ev, kick); break;
+    case 4: force_launch_tpp<4, STYLE>(s, boxes, u, grid, c, ev, kick); break;
+    default: force_launch_tpp<1, STYLE>(s, boxes, u, grid, c, ev, kick); break;
+    }
+}
+
+void launch_force(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev, int kick)
+{
+    const int grid = u.local.n < c.sms * 16 ? (u.local.n > 0 ? u.local.n : 1) : c.sms * 16;
+    if (c.style == 0) force_launch_style<0>(s, boxes, u, grid, c, ev, kick);
+    else force_launch_style<1>(s, boxes, u, grid, c, ev, kick);
+}
+
+// ---------------------------------------------------------------------------
+// thermo: per-unit kinetic energy / momentum partials, then per-box sums in unit order.
+// out[box*kPartialStride + q]: q=0 sum m v^2 (all), 1..6 virial, 7 pe, 8..10 momentum,
+// 11 sum m v^2 over the nve group.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kUnit) k_thermo_units(const BoxDesc *__restrict__ boxes,
+                                                        const Unit *__restrict__ units, int nunits)
+{
+    __shared__ double s_red[kUnit / 32][5];
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        const int c = B.st->cur;
+        const int i = U.begin + threadIdx.x;
+        double vals[5] = {0, 0, 0, 0, 0};
+        if (i < U.end) {
+            const int t = B.type[c][i];
+            const double m = B.mass[t - 1];
+            const double vx = B.v[c][0][i], vy = B.v[c][1][i], vz = B.v[c][2][i];
+            vals[0] = m * (vx * vx + vy * vy + vz * vz);
+            if (B.mask[c][i] & B.nve_bit) vals[4] = vals[0];
+            vals[1] = m * vx, vals[2] = m * vy, vals[3] = m * vz;
+        }
+#pragma unroll
+        for (int q = 0; q < 5; ++q)
+            for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_down_sync(0xffffffffu, vals[q], o);
+        if ((threadIdx.x & 31) == 0)
+            for (int q = 0; q < 5; ++q) s_red[threadIdx.x / 32][q] = vals[q];
+        __syncthreads();
+        if (threadIdx.x < 5) {
+            double a = 0.0;
+            for (int w = 0; w < kUnit / 32; ++w) a += s_red[w][threadIdx.x];
+            const int slot = threadIdx.x == 0 ? 0 : 7 + threadIdx.x;  // ke_all, px, py, pz, ke_group
+            B.partial[(size_t)(U.begin / kUnit) * kPartialStride + slot] = a;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_thermo_sum(const BoxDesc *__restrict__ boxes, int nbox, double *out)
+{
+    // one block per box: fixed-order tree over the unit partials
+    __shared__ double s[256];
+    const int b = blockIdx.x;
+    if (b >= nbox) return;
+    const BoxDesc &B = boxes[b];
+    const int nunit = (B.nlocal + kUnit - 1) / kUnit;
+    for (int q = 0; q < kPartialStride; ++q) {
+        double a = 0.0;
+        for (int k = threadIdx.x; k < nunit; k += blockDim.x) a += B.partial[(size_t)k * kPartialStride + q];
+        s[threadIdx.x] = a;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[(size_t)b * kPartialStride + q] = s[0];
+        __syncthreads();
+    }
+}
+
+void launch_thermo(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, double *out, int *)
+{
+    const int grid = u.local.n < 148 * 8 ? (u.local.n > 0 ? u.local.n : 1) : 148 * 8;
+    k_thermo_units<<<grid, kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
+    k_thermo_sum<<<u.nbox, 256, 0, s>>>(boxes, u.nbox, out);
+}
+
+// ---------------------------------------------------------------------------
+// density profile (fix density/meso, fix_density_profile_meso.cpp:118-151)
+// ---------------------------------------------------------------------------
+__global__ void k_density_profile(const BoxDesc *__restrict__ boxes, const Unit *__restrict__ units,
+                                  int nunits, int dim, int groupbit, double lo, double inv, int nbin,
+                                  unsigned long long *counts)
+{
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        const int c = B.st->cur;
+        const int i = U.begin + threadIdx.x;
+        if (i < U.end && (B.mask[c][i] & groupbit)) {
+            const int b = (int)floor((B.x[c][dim][i] - lo) * inv);
+            if (b >= 0 && b < nbin) atomicAdd(&counts[b], 1ull);
+        }
+    }
+}
+
+void launch_density_profile(cudaStream_t s, const BoxDesc *boxes, int, const Unit *units, int nunits,
+                            int dim, int groupbit, double lo, double inv, int nbin,
+                            unsigned long long *counts)
+{
+    const int grid = nunits < 148 * 8 ? (nunits > 0 ? nunits : 1) : 148 * 8;
+    k_density_profile<<<grid, kUnit, 0, s>>>(boxes, units, nunits, dim, groupbit, lo, inv, nbin, counts);
+}
+
+// ---------------------------------------------------------------------------
+// pair RNG on explicit signature pairs (test hook)
+// ---------------------------------------------------------------------------
+__global__ void k_gaussian(const uint32_t *si, const uint32_t *sj, double *exact, float *fast, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (exact) exact[i] = gaussian_exact(si[i], sj[i]);
+        if (fast) fast[i] = gaussian_fast(si[i], sj[i]);
+    }
+}
+
+void launch_gaussian(cudaStream_t s, const uint32_t *si, const uint32_t *sj, double *exact, float *fast, int n)
+{
+    const int grid = (n + 255) / 256 < 148 * 8 ? ((n + 255) / 256 > 0 ? (n + 255) / 256 : 1) : 148 * 8;
+    k_gaussian<<<grid, 256, 0, s>>>(si, sj, exact, fast, n);
+}
+
+}  // namespace mdpd

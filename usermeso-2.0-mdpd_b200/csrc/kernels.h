@@ -1,0 +1,60 @@
+// Host-side launchers of the device kernels.  Every launcher takes the device box table
+// and a device list of work units; grids are persistent (a multiple of the SM count).
+#pragma once
+
+#include "mdpd_dev.cuh"
+
+namespace mdpd {
+
+struct UnitList {
+    const Unit *d = nullptr;  // device array
+    int n = 0;
+};
+
+// units of one batch, by domain (all boxes concatenated)
+struct BatchUnits {
+    UnitList local;      // [0,nlocal) in chunks of kUnit, 32-aligned
+    UnitList all;        // [0,nlocal+ghost_cap) in chunks of kUnit
+    UnitList cls;        // [0,2*nbin) in chunks of 256 buckets
+    UnitList bins;       // [0,nbin) in chunks of 256 bins
+    UnitList scan_cls;   // [0,2*nbin) in chunks of kScanChunk
+    UnitList scan_ghost; // [0,nlocal+1)
+    UnitList scan_bin;   // [0,nbin)
+    int nbox = 0;
+};
+
+constexpr int kScanChunk = 2048;
+
+struct StepConfig {
+    int tpp_density = 1;   // threads per particle in the density pass
+    int tpp_force = 1;     // threads per particle in the force pass
+    int exact_rng = 0;     // FP64 bit-exact gaussian
+    int wall = 0;          // aboundary bounce-back in the integrate pass
+    int wall_coupling = 0; // phi-dependent gamma/sigma in the force pass
+    int style = 0;         // 0 mdpd, 1 dpd
+    int sms = 148;
+};
+
+// scratch counter words used for last-block detection (device)
+struct Counters {
+    int *integrate;
+    int *rebuild_last;
+};
+
+void launch_integrate(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c,
+                      int *done, cudaGraphConditionalHandle cond, int use_cond);
+void launch_force_rebuild_flag(cudaStream_t s, BoxDesc *boxes, int nbox, int value);
+void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c,
+                    int *done);
+void launch_density(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c);
+void launch_force(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev,
+                  int kick);
+void launch_thermo(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, double *out, int *done);
+void launch_density_profile(cudaStream_t s, const BoxDesc *boxes, int box, const Unit *units,
+                            int nunits, int dim, int groupbit, double lo, double inv, int nbin,
+                            unsigned long long *counts);
+// test hooks: the pair RNG on explicit signatures
+void launch_gaussian(cudaStream_t s, const uint32_t *si, const uint32_t *sj, double *exact,
+                     float *fast, int n);
+
+}  // namespace mdpd

@@ -1,0 +1,314 @@
+// Device-side types and helpers of the B200 mDPD/DPD timestep path.
+//
+// One BoxDesc per simulation box lives in device memory.  Every kernel takes the box
+// table plus a list of work units {box, begin, end}, so the same kernels step one box,
+// a batch of uneven boxes, or the boxes of a serving loop.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mdpd {
+
+constexpr int kMaxTypes = 8;
+constexpr int kUnit = 128;          // particles per work unit (multiple of 32)
+constexpr int kClassMax = 512;      // largest bucket the in-warp bucket sort accepts
+constexpr int kWarpsPerBlock = 8;
+
+// error bits reported per box (status word), mirrored by MDPD_ERR_* in include/mdpd.h
+enum : int {
+    kErrListOverflow = 1,   // a particle has more than n_col neighbours
+    kErrGhostOverflow = 2,  // more ghost images than the ghost capacity
+    kErrBucketOverflow = 4, // a bin or reorder bucket holds more than kClassMax particles
+    kErrNonFinite = 8,      // NaN/Inf force
+    kErrLost = 16,          // particle outside the box by more than one period
+};
+
+struct PairCoeff {  // per type pair; FP32 pair arithmetic
+    float cut, cutsq, inv_cut, cut_r, inv_cut_r;
+    float A, B, gamma, sigma;  // mdpd: A (attractive), B (repulsive); dpd: A = a0
+    float expw;
+    float e_cut, e_cut_r;     // energy prefactors 0.5*A*cut, 0.5*B*cut_r
+};
+
+struct Unit {
+    int box, begin, end;
+};
+
+// device-resident per-box scalars, updated by kernels
+struct BoxState {
+    long long step;        // last completed timestep
+    int ago;               // steps since last neighbor build
+    int moved;             // some particle moved more than skin/2 (this step)
+    int rebuild;           // rebuild decided for this step
+    int nghost;
+    int n_bulk;            // locals before the first border particle
+    int status;            // error bits
+    int max_count;         // largest neighbour count at the last build
+    long long nbuild;
+    int cur;               // live copy of the double-buffered arrays
+    int pad;
+};
+
+struct BoxDesc {
+    // ---- geometry ----
+    double lo[3], hi[3], prd[3], cen[3];
+    double binsize[3], bininv[3], coord_inv[3];
+    double cutghost, triggersq;
+    float rc2_tail;
+    int mbin[3], nbin;
+    int l1_shift;
+    int nlocal, nrow, ghost_cap, n_col;
+    int every, delay, check;
+    // ---- physics ----
+    int style;   // 0 mdpd, 1 dpd
+    int ntype;
+    int exact_rng;
+    PairCoeff coeff[kMaxTypes * kMaxTypes];
+    double dtfm[kMaxTypes];  // 0.5*dt*ftm2v * rcp(mass)
+    double mass[kMaxTypes];
+    double dtv;
+    float dt_inv_sqrt;
+    uint32_t seed;
+    int nve_bit;
+    int rho_bit;
+    float cut_rho, rho_factor;   // 15/(2 pi cut_rho^5)
+    int body_bit;
+    float body[3];
+    int arb_bc, mobile_bit, wall_bit;   // wall coupling (pair_style mdpd/meso ... fluid wall)
+    int wall_fix;                        // aboundary bounce-back active
+    float cut_phi, phi_factor, dw_factor, phi_c;
+    double dtf;
+    // ---- per-particle arrays (locals), double-buffered for the reorder: the live copy
+    //      is [st->cur], the other receives the permuted state at a rebuild ----
+    double *x[2][3], *v[2][3], *xh[3];
+    float4 *f[2];
+    int *tag[2], *type[2], *mask[2];
+    // ---- packed FP32 state, locals then ghosts ----
+    float4 *pos, *vel;
+    float *rho;           // locals then ghosts
+    float *phi[2];        // wall volume fraction of locals (double-buffered with x)
+    int *gsrc, *gimg, *gfirst;
+    // ---- neighbour list (locally transposed: 32-row blocks) ----
+    int *count, *table;
+    // ---- rebuild scratch ----
+    int *bin_rank;        // Morton rank of each bin (reorder class order)
+    int *cls_count, *cls_start, *cls_cursor;  // 2*nbin
+    int *cls_of;          // class of each local
+    int *sub_of;          // secondary key of each local
+    int *perm;            // new -> old
+    int *bin_of;          // bin of locals+ghosts
+    int *bin_count, *bin_start, *bin_cursor;  // nbin (+1)
+    int *bin_order;       // bin-sorted particle indices
+    float4 *bpos;         // positions in bin order
+    int *scan_part;       // per-chunk partial sums for scans
+    // ---- thermo partials ----
+    double *partial;      // per unit: [ke, vir_xx, vir_yy, vir_zz, vir_xy, vir_xz, vir_yz, pe, px, py, pz]
+    BoxState *st;
+};
+
+constexpr int kPartialStride = 12;
+
+// ---------------------------------------------------------------------------
+// counter-based RNG (TEA, GPU variant of Zafar et al.) and the reference's
+// own gaussian transform, restated so the FP64 value is bit-identical.
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ void tea_core(uint32_t &v0, uint32_t &v1, int rounds)
+{
+    uint32_t sum = 0;
+#pragma unroll
+    for (int r = 0; r < rounds; ++r) {
+        sum += 0x9E3779B9u;
+        v0 += ((v1 << 4) + 0xA341316Cu) ^ (v1 + sum) ^ ((v1 >> 5) + 0xC8013EA4u);
+        v1 += ((v0 << 4) + 0xAD90777Du) ^ (v0 + sum) ^ ((v0 >> 5) + 0x7E95761Eu);
+    }
+}
+
+template <int N> __host__ __device__ __forceinline__ uint32_t premix_tea(uint32_t v0, uint32_t v1)
+{
+    tea_core(v0, v1, N);
+    return v0 ^ v1;
+}
+
+__host__ __device__ __forceinline__ uint32_t brev32(uint32_t x)
+{
+#ifdef __CUDA_ARCH__
+    return __brev(x);
+#else
+    uint32_t r = 0;
+    for (int i = 0; i < 32; ++i) r |= ((x >> i) & 1u) << (31 - i);
+    return r;
+#endif
+}
+
+__host__ __device__ __forceinline__ uint64_t spread3(uint32_t x)
+{
+    uint64_t r = x & 0x1FFFFFu;
+    r = (r | (r << 32)) & 0x1F00000000FFFFull;
+    r = (r | (r << 16)) & 0x1F0000FF0000FFull;
+    r = (r | (r << 8)) & 0x100F00F00F00F00Full;
+    r = (r | (r << 4)) & 0x10C30C30C30C30C3ull;
+    r = (r | (r << 2)) & 0x1249249249249249ull;
+    return r;
+}
+
+__host__ __device__ __forceinline__ uint64_t morton3(uint32_t x, uint32_t y, uint32_t z)
+{
+    return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
+}
+
+// seed of the current step: premix_TEA<64>(seed, step)
+__host__ __device__ __forceinline__ uint32_t seed_now(uint32_t seed, long long step)
+{
+    return premix_tea<64>(seed, (uint32_t)step);
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ uint32_t sig_mdpd(int tag, uint32_t sn)
+{
+    return premix_tea<32>(brev32((uint32_t)tag), sn);
+}
+
+__device__ __forceinline__ uint32_t sig_dpd(int tag, float vx, float vy, float vz, uint32_t sn)
+{
+    uint32_t a = (__float_as_uint(vx) & 0x7FF000u) >> 12;
+    uint32_t b = (__float_as_uint(vy) & 0x7FF000u) >> 12;
+    uint32_t c = (__float_as_uint(vz) & 0x7FF000u) >> 12;
+    return sn ^ premix_tea<16>(brev32((uint32_t)tag), (uint32_t)morton3(a, b, c));
+}
+
+// reciprocal by magic seed + 4 Newton steps, each step one FMA pair
+__host__ __device__ __forceinline__ double rcp_newton(double x)
+{
+#ifdef __CUDA_ARCH__
+    double xinv = __longlong_as_double(0x7FDE62361B1C4042LL - __double_as_longlong(x));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        double e = __fma_rn(x, xinv, -1.0);
+        xinv = __fma_rn(-e, xinv, xinv);
+    }
+    return xinv;
+#else
+    union { double d; long long l; } u;
+    u.d = x;
+    u.l = 0x7FDE62361B1C4042LL - u.l;
+    double xinv = u.d;
+    for (int k = 0; k < 4; ++k) {
+        double e = __builtin_fma(x, xinv, -1.0);
+        xinv = __builtin_fma(-e, xinv, xinv);
+    }
+    return xinv;
+#endif
+}
+
+__device__ __forceinline__ double rsqrt_newton(double x)
+{
+    double r = __longlong_as_double(0x5FE660FCB5422422LL - (__double_as_longlong(x) >> 1));
+    double x2m = __dmul_rn(x, -0.5);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) r = __dmul_rn(r, __fma_rn(__dmul_rn(r, r), x2m, 1.5));
+    return r;
+}
+
+// log2(x * 2^-32) for x >= 1 with the reference's 8th-order polynomial
+__device__ __forceinline__ double log2u_exact(uint32_t x)
+{
+    int I = 31 - __clz(x);
+    double xm = __dmul_rn((double)x, __longlong_as_double((long long)(1023 - I) << 52));
+    bool pred = xm > 1.4142135623730950488;
+    xm = __dmul_rn(xm, pred ? 0.5 : 7.0710678118654757274E-1);
+    double z = __dmul_rn(__dadd_rn(xm, -1.0), rcp_newton(__dadd_rn(xm, 1.0)));
+    double y = __dmul_rn(__dmul_rn(z, z), 33.9705627484771406);
+    double s = 2.55854634203511155E-7;
+    s = __fma_rn(s, y, 1.05013262724846015E-5);
+    s = __fma_rn(s, y, 5.00072802051539862E-4);
+    s = __fma_rn(s, y, 2.83126505877817866E-2);
+    s = __fma_rn(s, y, 2.88539008179006374E+0);
+    return __fma_rn(z, s, __dadd_rn(pred ? 1.0 : 0.5, (double)(I - 32)));
+}
+
+__device__ __forceinline__ double cospi_exact(double x)
+{
+    x = __fma_rn(2.0, x, -1.0);  // exact: 2x is exact
+    double x2 = __dmul_rn(x, x);
+    double s = 3.41817283473266926E-6;
+    s = __fma_rn(s, x2, -1.60217135750921262E-4);
+    s = __fma_rn(s, x2, 4.68162024021793872E-3);
+    s = __fma_rn(s, x2, -7.96925872866600517E-2);
+    s = __fma_rn(s, x2, 6.45964092644060746E-1);
+    s = __fma_rn(s, x2, -1.57079632662144460E+0);
+    return __dmul_rn(s, x);
+}
+
+// bit-exact FP64 pairwise gaussian from two signatures (symmetric in i,j)
+__device__ __forceinline__ double gaussian_exact(uint32_t si, uint32_t sj)
+{
+    uint32_t v0 = max(si, sj), v1 = min(si, sj);
+    tea_core(v0, v1, 4);
+    double f = __dmul_rn(cospi_exact(__dmul_rn((double)(v0 & 0x7FFFFFFFu), 4.6566128730773925781E-10)),
+                         (v0 & 0x80000000u) ? 1.0 : -1.0);
+    double a = __dmul_rn(-2.0 * 6.9314718055994528623E-1, log2u_exact(max(v1, 1u)));
+    double r = __dmul_rn(a, rsqrt_newton(a));
+    double g = __dmul_rn(r, f);
+    return fmax(-4.0, fmin(g, 4.0));
+}
+
+// FP32 transform of the same TEA words (same polynomial for the angle, libm log2f)
+__device__ __forceinline__ float gaussian_fast(uint32_t si, uint32_t sj)
+{
+    uint32_t v0 = max(si, sj), v1 = min(si, sj);
+    tea_core(v0, v1, 4);
+    float x = __fmaf_rn(2.0f, (float)(v0 & 0x7FFFFFFFu) * 4.6566128730773926e-10f, -1.0f);
+    float x2 = x * x;
+    float s = 3.41817283473266926E-6f;
+    s = __fmaf_rn(s, x2, -1.60217135750921262E-4f);
+    s = __fmaf_rn(s, x2, 4.68162024021793872E-3f);
+    s = __fmaf_rn(s, x2, -7.96925872866600517E-2f);
+    s = __fmaf_rn(s, x2, 6.45964092644060746E-1f);
+    s = __fmaf_rn(s, x2, -1.57079632662144460E+0f);
+    float f = (v0 & 0x80000000u) ? s * x : -s * x;
+    float l = log2f((float)max(v1, 1u)) - 32.0f;
+    float r = sqrtf(fmaxf((float)(-2.0 * 6.9314718055994528623E-1) * l, 0.0f));
+    return fmaxf(-4.0f, fminf(r * f, 4.0f));
+}
+
+// squared distance with the contraction nvcc applies to dx*dx + dy*dy + dz*dz
+__device__ __forceinline__ float dist2(float dx, float dy, float dz)
+{
+    return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+}
+
+// entry k of particle i in the locally transposed table
+__device__ __forceinline__ int list_addr(int i, int k, int n_col)
+{
+    return ((i & ~31) + (k & 31)) * n_col + (k & ~31) + (i & 31);
+}
+
+__device__ __forceinline__ int clamp_bin(int i, int nmax)
+{
+    return max(0, min(i, nmax - 1));
+}
+
+// (x - lo) * inv + 1.0 contracted into one FMA and truncated, as the reference's binning
+__device__ __forceinline__ int bin_coord(double x, double lo, double inv)
+{
+    return (int)__fma_rn(__dsub_rn(x, lo), inv, 1.0);
+}
+
+__device__ __forceinline__ int ptype(const float4 &p) { return __float_as_int(p.w) & 0xFF; }
+__device__ __forceinline__ int pflags(const float4 &p) { return __float_as_int(p.w) >> 8; }
+
+// packed .w word of a position: type-1 in bits 0-7, mobile bit 8, wall bit 9
+__device__ __forceinline__ float pack_w(const BoxDesc &B, int type, int mask)
+{
+    int w = (type - 1) & 0xFF;
+    if (B.arb_bc) {
+        if (mask & B.mobile_bit) w |= 1 << 8;
+        if (mask & B.wall_bit) w |= 1 << 9;
+    }
+    return __int_as_float(w);
+}
+
+#endif  // __CUDACC__
+
+}  // namespace mdpd

@@ -1,0 +1,400 @@
+// Serving loop: jobs (boxes + step counts) are admitted while their device footprint fits
+// the HBM budget, stay resident until done, and are stepped together by the batched graph.
+// Arrivals and retirements change the batch between chunks of steps (continuous batching).
+// One driver thread issues all device work; submit/poll/cancel only touch the queue.
+//
+// The reference's only form of many simulations is one LAMMPS instance per MPI rank
+// group (main_ensemble, src/main.cpp:49-117); here they share one GPU and one launch.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+
+#include "../../include/mdpd.h"
+#include "engine.h"
+#include "script.h"
+
+namespace mdpd {
+void spec_from_box(const mdpd_box_spec &bs, Spec &s, Particles &p);
+}
+
+using namespace mdpd;
+
+namespace {
+
+struct Job {
+    int64_t id = 0;
+    mdpd_job_spec spec{};
+    std::vector<double> x0, v0;  // copies of caller-provided initial state
+    int state = 0, error = 0;
+    int64_t done = 0;
+    double submit_s = 0, start_s = 0, end_s = 0;
+    std::vector<float> step_ms;
+    mdpd_thermo_t thermo{};
+    std::vector<double> xf, vf;
+    std::unique_ptr<Box> box;
+    size_t bytes = 0;
+    bool cancel = false;
+};
+
+double pct(std::vector<float> v, double p)
+{
+    if (v.empty()) return 0;
+    std::sort(v.begin(), v.end());
+    const size_t k = std::min(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5));
+    return v[k];
+}
+
+}  // namespace
+
+struct mdpd_server_s {
+    uint64_t budget = 0;
+    int device = 0;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::map<int64_t, std::shared_ptr<Job>> jobs;
+    std::deque<int64_t> queue;
+    int64_t next_id = 1;
+    bool stop = false;
+    std::thread th;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    // stats
+    double particle_steps = 0, busy_s = 0;
+    std::vector<float> all_step_ms;
+    std::vector<double> job_latency_s;
+    uint64_t resident = 0, peak_resident = 0;
+    int chunk = 50;
+
+    double now() const
+    {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+
+    void loop();
+};
+
+void mdpd_server_s::loop()
+{
+    cudaSetDevice(device);
+    std::vector<std::shared_ptr<Job>> active;
+    std::unique_ptr<Batch> batch;
+    StepConfig cfg;
+    cfg.sms = sm_count();
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (;;) {
+        std::vector<std::shared_ptr<Job>> admitted;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            if (active.empty()) cv.wait(lk, [&] { return stop || !queue.empty(); });
+            if (stop) break;
+            // admission: FIFO while the next job fits the budget
+            while (!queue.empty()) {
+                std::shared_ptr<Job> j = jobs[queue.front()];
+                if (j->cancel) {
+                    j->state = 4;
+                    queue.pop_front();
+                    continue;
+                }
+                if (resident + j->bytes > budget) break;
+                queue.pop_front();
+                resident += j->bytes;
+                admitted.push_back(j);
+            }
+        }
+        // allocate admitted boxes (outside the lock)
+        std::vector<int> fresh;
+        for (auto &j : admitted) {
+            try {
+                Spec s;
+                Particles p;
+                mdpd_box_spec bs = j->spec.box;
+                if (!j->x0.empty()) {
+                    bs.x = j->x0.data();
+                    bs.v = j->v0.empty() ? nullptr : j->v0.data();
+                }
+                spec_from_box(bs, s, p);
+                j->box.reset(new Box(s, p, cfg.sms));
+                std::lock_guard<std::mutex> lk(mu);
+                j->state = 1;
+                j->start_s = now();
+                active.push_back(j);
+            } catch (const std::exception &e) {
+                std::lock_guard<std::mutex> lk(mu);
+                j->state = 3;
+                j->error = std::string(e.what()).rfind("OOM", 0) == 0 ? MDPD_ERR_OOM : MDPD_ERR_ARG;
+                j->end_s = now();
+                resident -= j->bytes;
+            }
+        }
+        peak_resident = std::max(peak_resident, resident);
+        if (active.empty()) continue;
+        const bool changed = !admitted.empty() || !batch;
+        if (changed) {
+            batch.reset();
+            std::vector<Box *> raw;
+            for (auto &j : active) raw.push_back(j->box.get());
+            cfg.style = active[0]->spec.box.style;
+            try {
+                batch.reset(new Batch(raw, cfg));
+                for (size_t k = 0; k < active.size(); ++k)
+                    if (std::find(admitted.begin(), admitted.end(), active[k]) != admitted.end())
+                        fresh.push_back((int)k);
+                batch->setup_boxes(fresh);
+            } catch (const std::exception &e) {
+                std::lock_guard<std::mutex> lk(mu);
+                for (auto &j : active) {
+                    j->state = 3;
+                    j->error = MDPD_ERR_CUDA;
+                    j->end_s = now();
+                    j->box.reset();
+                }
+                active.clear();
+                batch.reset();
+                resident = 0;
+                continue;
+            }
+        }
+        // run a chunk: until the first job finishes, at most `chunk` steps
+        int64_t k = chunk;
+        for (auto &j : active) k = std::min<int64_t>(k, j->spec.nsteps - j->done);
+        k = std::max<int64_t>(k, 1);
+        cudaEventRecord(e0, batch->stream());
+        batch->run(k, false);
+        cudaEventRecord(e1, batch->stream());
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        std::string msg;
+        const int st = batch->status(msg);
+        long long nparts = 0;
+        for (auto &j : active) nparts += j->box->n;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            particle_steps += (double)nparts * k;
+            busy_s += ms * 1e-3;
+            for (int64_t q = 0; q < k; ++q) all_step_ms.push_back(ms / k);
+        }
+        // retire finished / failed / cancelled jobs
+        std::vector<std::shared_ptr<Job>> keep;
+        bool retired = false;
+        std::vector<Thermo> th;
+        for (size_t q = 0; q < active.size(); ++q) {
+            auto &j = active[q];
+            const BoxState bst = j->box->state();
+            j->done += k;
+            for (int64_t s = 0; s < k; ++s) j->step_ms.push_back(ms / k);
+            const bool fail = bst.status != 0;
+            if (j->done >= j->spec.nsteps || fail || j->cancel) {
+                if (th.empty()) batch->thermo(th);
+                Thermo t = th[q];
+                mdpd_thermo_t out{};
+                out.step = t.step;
+                out.natoms = t.n;
+                out.nbuild = t.nbuild;
+                out.temp = t.temp;
+                out.press = t.press;
+                out.ke = 0.5 * t.ke_all;
+                for (int d = 0; d < 3; ++d) out.momentum[d] = t.mom[d];
+                out.status = t.status;
+                std::vector<double> xf, vf;
+                if (j->spec.keep_state && !fail) {
+                    const int n = j->box->n;
+                    std::vector<double> xi(3 * (size_t)n), vi(3 * (size_t)n);
+                    std::vector<int32_t> tag(n);
+                    j->box->download_state(xi.data(), vi.data(), nullptr, tag.data(), nullptr, nullptr);
+                    xf.resize(3 * (size_t)n);
+                    vf.resize(3 * (size_t)n);
+                    for (int i = 0; i < n; ++i)
+                        for (int d = 0; d < 3; ++d) {
+                            xf[3 * (tag[i] - 1) + d] = xi[3 * i + d];
+                            vf[3 * (tag[i] - 1) + d] = vi[3 * i + d];
+                        }
+                }
+                std::lock_guard<std::mutex> lk(mu);
+                j->thermo = out;
+                j->xf.swap(xf);
+                j->vf.swap(vf);
+                j->state = fail ? 3 : j->cancel ? 4 : 2;
+                if (fail) j->error = (bst.status & kErrNonFinite) ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW;
+                j->end_s = now();
+                job_latency_s.push_back(j->end_s - j->submit_s);
+                resident -= j->bytes;
+                retired = true;
+            } else
+                keep.push_back(j);
+        }
+        (void)st;
+        if (retired) {
+            batch.reset();
+            for (auto &j : active)
+                if (std::find(keep.begin(), keep.end(), j) == keep.end()) j->box.reset();
+            active.swap(keep);
+            cv.notify_all();
+        }
+    }
+    batch.reset();
+    for (auto &j : active) j->box.reset();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+extern "C" {
+
+int mdpd_box_bytes(const mdpd_box_spec *spec, uint64_t *bytes)
+{
+    if (!spec || !bytes || spec->n <= 0) return MDPD_ERR_ARG;
+    try {
+        Spec sp;
+        Particles p;
+        mdpd_box_spec bs = *spec;
+        bs.x = nullptr, bs.v = nullptr;
+        bs.n = 1;
+        spec_from_box(bs, sp, p);
+        *bytes = Box::estimate_bytes(sp, spec->n);
+    } catch (const std::exception &) {
+        return MDPD_ERR_ARG;
+    }
+    return MDPD_OK;
+}
+
+int mdpd_server_start(mdpd_server_t **out, uint64_t budget, const mdpd_opts *opts)
+{
+    if (!out || budget == 0) return MDPD_ERR_ARG;
+    auto *s = new mdpd_server_s;
+    s->budget = budget;
+    s->device = opts ? opts->device : 0;
+    s->th = std::thread([s] { s->loop(); });
+    *out = s;
+    return MDPD_OK;
+}
+
+int mdpd_server_submit(mdpd_server_t *s, const mdpd_job_spec *job, int64_t *id)
+{
+    if (!s || !job || !id || job->nsteps <= 0 || job->box.n <= 0) return MDPD_ERR_ARG;
+    auto j = std::make_shared<Job>();
+    j->spec = *job;
+    const int n = job->box.n;
+    if (job->box.x) j->x0.assign(job->box.x, job->box.x + 3 * (size_t)n);
+    if (job->box.v) j->v0.assign(job->box.v, job->box.v + 3 * (size_t)n);
+    j->spec.box.x = nullptr;
+    j->spec.box.v = nullptr;
+    try {
+        Spec sp;
+        Particles p;
+        mdpd_box_spec bs = job->box;
+        bs.x = nullptr, bs.v = nullptr;
+        bs.n = 1;  // geometry/physics check only; the footprint uses the real n
+        spec_from_box(bs, sp, p);
+        j->bytes = Box::estimate_bytes(sp, n);
+    } catch (const std::exception &) {
+        return MDPD_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (j->bytes > s->budget) return MDPD_ERR_BUDGET;
+    j->id = s->next_id++;
+    j->submit_s = s->now();
+    s->jobs[j->id] = j;
+    s->queue.push_back(j->id);
+    *id = j->id;
+    s->cv.notify_all();
+    return MDPD_OK;
+}
+
+int mdpd_server_poll(mdpd_server_t *s, int64_t id, mdpd_job_result *out)
+{
+    if (!s || !out) return MDPD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return MDPD_ERR_ARG;
+    const Job &j = *it->second;
+    std::memset(out, 0, sizeof(*out));
+    out->state = j.state;
+    out->error = j.error;
+    out->steps_done = j.done;
+    out->submit_s = j.submit_s;
+    out->start_s = j.start_s;
+    out->end_s = j.end_s;
+    out->step_ms_p50 = pct(j.step_ms, 0.5);
+    out->step_ms_p99 = pct(j.step_ms, 0.99);
+    out->thermo = j.thermo;
+    return MDPD_OK;
+}
+
+int mdpd_server_get_state(mdpd_server_t *s, int64_t id, double *x, double *v, int64_t n)
+{
+    if (!s) return MDPD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return MDPD_ERR_ARG;
+    const Job &j = *it->second;
+    if (j.state != 2 || j.xf.empty()) return MDPD_ERR_STATE;
+    if ((int64_t)j.xf.size() != 3 * n) return MDPD_ERR_ARG;
+    if (x) std::copy(j.xf.begin(), j.xf.end(), x);
+    if (v) std::copy(j.vf.begin(), j.vf.end(), v);
+    return MDPD_OK;
+}
+
+int mdpd_server_cancel(mdpd_server_t *s, int64_t id)
+{
+    if (!s) return MDPD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return MDPD_ERR_ARG;
+    it->second->cancel = true;
+    s->cv.notify_all();
+    return MDPD_OK;
+}
+
+int mdpd_server_drain(mdpd_server_t *s, double timeout_s)
+{
+    if (!s) return MDPD_ERR_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto pending = [&] {
+        for (auto &kv : s->jobs)
+            if (kv.second->state < 2) return true;
+        return false;
+    };
+    if (timeout_s > 0) {
+        if (!s->cv.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return !pending(); }))
+            return MDPD_ERR_TIMEOUT;
+    } else
+        s->cv.wait(lk, [&] { return !pending(); });
+    return MDPD_OK;
+}
+
+int mdpd_server_stats(mdpd_server_t *s, double *o)
+{
+    if (!s || !o) return MDPD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    o[0] = s->busy_s > 0 ? s->particle_steps / s->busy_s : 0;
+    o[1] = pct(s->all_step_ms, 0.5);
+    o[2] = pct(s->all_step_ms, 0.99);
+    std::vector<float> lat(s->job_latency_s.begin(), s->job_latency_s.end());
+    o[3] = pct(lat, 0.5);
+    o[4] = pct(lat, 0.99);
+    o[5] = (double)s->job_latency_s.size();
+    o[6] = (double)s->peak_resident;
+    return MDPD_OK;
+}
+
+void mdpd_server_stop(mdpd_server_t *s)
+{
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv.notify_all();
+    }
+    if (s->th.joinable()) s->th.join();
+    delete s;
+}
+
+}  // extern "C"
