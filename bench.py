@@ -95,6 +95,19 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def aggregate(particle_steps, seconds, world, device="cuda"):
+    """Whole-job throughput over ranks: particle-steps summed, time = max over ranks."""
+    if world == 1:
+        return particle_steps / seconds, seconds
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    p = torch.tensor([particle_steps], dtype=torch.float64, device=device)
+    dist.all_reduce(p, op=dist.ReduceOp.SUM)
+    return float(p.item()) / float(t.item()), float(t.item())
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -188,20 +201,6 @@ def main():
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
-
     # ---- headline: batched 256-box workload, resident in HBM -------------------------------
     cfg = config4(seed=1 + rank)
     specs = specs_of(cfg)
@@ -216,8 +215,7 @@ def main():
         ms = b.time(args.steps)              # CUDA events on the batch stream, K steps
         barrier()
     r1 = b.rebuild_steps()
-    t_max = max_over_ranks(ms * args.steps / 1e3)
-    value = sum_over_ranks(ntot * args.steps) / t_max
+    value, t_max = aggregate(ntot * args.steps, ms * args.steps / 1e3, world)
     gpu_launches = 3 * args.steps + 17 * (r1 - r0)
     b.close()
 

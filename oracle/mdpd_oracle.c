@@ -151,8 +151,10 @@ static double ref_log2u(uint32_t x)
     double xm = (double)x * pow2i(-I);
     double ex = (double)(I - 32);
     int pred = xm > 1.4142135623730950488;
-    xm *= pred ? 0.5 : 7.0710678118654757274E-1;
-    double z = (xm - 1.0) * orc_rcp(xm + 1.0);
+    /* x *= m; z = (x-1)*rcp(x+1): nvcc fuses the scale into both uses (pinned against the
+     * reference header's device code in tests/golden/ref_device.json) */
+    const double m = pred ? 0.5 : 7.0710678118654757274E-1;
+    double z = fma(xm, m, -1.0) * orc_rcp(fma(xm, m, 1.0));
     double y = z * z * 33.9705627484771406;
     double s = c4;
     s = fma(s, y, c3);

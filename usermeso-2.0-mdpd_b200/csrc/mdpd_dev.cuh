@@ -216,8 +216,10 @@ __device__ __forceinline__ double log2u_exact(uint32_t x)
     int I = 31 - __clz(x);
     double xm = __dmul_rn((double)x, __longlong_as_double((long long)(1023 - I) << 52));
     bool pred = xm > 1.4142135623730950488;
-    xm = __dmul_rn(xm, pred ? 0.5 : 7.0710678118654757274E-1);
-    double z = __dmul_rn(__dadd_rn(xm, -1.0), rcp_newton(__dadd_rn(xm, 1.0)));
+    // the scale into [1/sqrt2, sqrt2) is fused into both x-1 and x+1, as the reference's
+    // compiled code does
+    const double m = pred ? 0.5 : 7.0710678118654757274E-1;
+    double z = __dmul_rn(__fma_rn(xm, m, -1.0), rcp_newton(__fma_rn(xm, m, 1.0)));
     double y = __dmul_rn(__dmul_rn(z, z), 33.9705627484771406);
     double s = 2.55854634203511155E-7;
     s = __fma_rn(s, y, 1.05013262724846015E-5);
@@ -253,22 +255,27 @@ __device__ __forceinline__ double gaussian_exact(uint32_t si, uint32_t sj)
     return fmax(-4.0, fmin(g, 4.0));
 }
 
-// FP32 transform of the same TEA words (same polynomial for the angle, libm log2f)
+// FP32 transform of the same TEA words (same polynomial for the angle; log of the radius
+// word through log1pf near 2^32 so a tiny radius keeps its relative accuracy)
 __device__ __forceinline__ float gaussian_fast(uint32_t si, uint32_t sj)
 {
     uint32_t v0 = max(si, sj), v1 = min(si, sj);
     tea_core(v0, v1, 4);
-    float x = __fmaf_rn(2.0f, (float)(v0 & 0x7FFFFFFFu) * 4.6566128730773926e-10f, -1.0f);
-    float x2 = x * x;
+    // 2u - 1 with u = (v0 & 0x7fffffff) * 2^-31, formed as (w - 2^30) * 2^-30 (one rounding)
+    const float x = (float)((int)(v0 & 0x7FFFFFFFu) - (1 << 30)) * 9.3132257461547852e-10f;
+    const float x2 = x * x;
     float s = 3.41817283473266926E-6f;
     s = __fmaf_rn(s, x2, -1.60217135750921262E-4f);
     s = __fmaf_rn(s, x2, 4.68162024021793872E-3f);
     s = __fmaf_rn(s, x2, -7.96925872866600517E-2f);
     s = __fmaf_rn(s, x2, 6.45964092644060746E-1f);
     s = __fmaf_rn(s, x2, -1.57079632662144460E+0f);
-    float f = (v0 & 0x80000000u) ? s * x : -s * x;
-    float l = log2f((float)max(v1, 1u)) - 32.0f;
-    float r = sqrtf(fmaxf((float)(-2.0 * 6.9314718055994528623E-1) * l, 0.0f));
+    const float f = (v0 & 0x80000000u) ? s * x : -s * x;
+    const uint32_t w = max(v1, 1u);
+    // log2(w * 2^-32): log1p of the (exact) distance to 2^32 in the upper half
+    const float l = w >= 0x80000000u ? log1pf(-(float)(0u - w) * 2.3283064365386963e-10f) * 1.4426950408889634f
+                                     : log2f((float)w) - 32.0f;
+    const float r = sqrtf(fmaxf((float)(-2.0 * 6.9314718055994528623E-1) * l, 0.0f));
     return fmaxf(-4.0f, fminf(r * f, 4.0f));
 }
 
