@@ -181,6 +181,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours")
+    ap.add_argument("--equil", type=int, default=300, help="untimed equilibration steps from the random start")
     ap.add_argument("--no-extras", action="store_true", help="skip plain/served/roofline/cpu legs")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0")); world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -207,6 +208,7 @@ def main():
     ntot = sum(c["n"] for c in cfg)
     b = mdpd.Batch(specs, device=local)
     b.setup()
+    b.step(args.equil)  # relax the random start (untimed)
     b.step(args.warmup)
     r0 = b.rebuild_steps()
     barrier()
@@ -217,6 +219,7 @@ def main():
     r1 = b.rebuild_steps()
     value, t_max = aggregate(ntot * args.steps, ms * args.steps / 1e3, world)
     gpu_launches = 3 * args.steps + 17 * (r1 - r0)
+    eq_states = [b.state(k) for k in range(len(cfg))] if (not args.no_extras and rank == 0) else None
     b.close()
 
     line = {"metric": "mDPD particle-steps/s (batched 256-box workload)", "value": value,
@@ -224,6 +227,8 @@ def main():
             "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 pair / f64 integrate", "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD, "boxes": 256, "particles_per_gpu": ntot,
+                       "start": f"uniform random positions, Maxwell velocities, {args.equil} untimed steps",
+                       "rebuild_steps_timed": r1 - r0,
                        "l2": "inputs larger than L2: state + lists of ~%d particles (%.1f GB)" % (
                            ntot, ntot * 1.1e-6),
                        "parallelism": f"replicas x{world} (independent box sets)"},
@@ -231,11 +236,8 @@ def main():
 
     if not args.no_extras and rank == 0:
         # ---- e2e through the C ABI: host arrays in, K steps, host arrays out ----------------
-        rng = np.random.default_rng(11)
-        xs, vs = [], []
-        for c in cfg:
-            xs.append(rng.uniform(0, c["L"], (c["n"], 3)))
-            v = rng.normal(0, 1, (c["n"], 3)); vs.append(v - v.mean(0))
+        xs = [x for x, _ in eq_states]
+        vs = [v for _, v in eq_states]
         t0 = time.perf_counter()
         sp = [mdpd.box_spec(c["n"], c["L"], A=c["A"], B=c["B"], cut_r=c["rd"], seed=c["seed"], x=x, v=v)
               for c, x, v in zip(cfg, xs, vs)]
@@ -255,7 +257,8 @@ def main():
 
         # ---- plain single-box path on the same boxes (one box per launch sequence) ----------
         plain_ps, plain_s = 0.0, 0.0
-        for s, c in zip(specs_of(cfg), cfg):
+        for c, x, v in zip(cfg, xs, vs):
+            s = mdpd.box_spec(c["n"], c["L"], A=c["A"], B=c["B"], cut_r=c["rd"], seed=c["seed"], x=x, v=v)
             bb = mdpd.Batch([s], device=local)
             bb.setup()
             bb.step(3)
@@ -272,6 +275,7 @@ def main():
         s4 = mdpd.box_spec(n4, (n4 / RHO) ** (1 / 3), A=-40.0, B=25.0, seed=4242, init_seed=99)
         b4 = mdpd.Batch([s4], device=local)
         b4.setup()
+        b4.step(args.equil)
         b4.step(args.warmup)
         prof = b4.profile(max(10, args.steps // 2))
         ms4 = b4.time(max(10, args.steps // 2))

@@ -52,6 +52,8 @@ typedef struct mdpd_thermo_t {
     double virial[6];     /* xx yy zz xy xz yz, sums of the per-atom halved virials */
     double momentum[3];
     double temp_group;    /* temperature of the nve/meso group */
+    double ptensor[6];    /* pressure tensor (kinetic + virial)/V: xx yy zz xy xz yz */
+    double surface_tension; /* (Lx/2)(Pxx - (Pyy+Pzz)/2) for a slab normal to x */
     int32_t status;       /* device error bits */
     int32_t pad;
 } mdpd_thermo_t;
@@ -84,6 +86,7 @@ void mdpd_destroy(mdpd_t *h);
  * name: "pos4" (float4, locals+ghosts), "vel4" (float4, locals+ghosts), "rho" (float,
  * locals+ghosts), "force" (float4, locals), "count" (int, locals), "tag" (int, locals),
  * "ghost_src" (int), "ghost_img" (int), "x" (double 3*n, locals, internal order),
+ * "phi" (float, locals: wall volume fraction of fix aboundary/rho/meso),
  * "list" (int, n_col*ceil32(n): the locally transposed table, neigh_list_meso.cu:143-147).
  * sizes: returns the element count of a field in *count.                                 */
 int mdpd_field_size(mdpd_t *h, const char *name, int64_t *count);

@@ -228,6 +228,25 @@ def force_dpd(pos4, vel4, count, table, coeffs, dt, ev=False):
     return (f, vir, ep) if ev else f
 
 
+def aboundary(x, v, xa, mask_all, count, table, mobile_bit, wall_bit, cut_phi, rho_wall, phi_c, dt,
+              mass_type, types):
+    """Wall volume fraction + bounce-back of mobile locals (gpu_aboundary); returns x, v, phi."""
+    n = len(count)
+    xs = [np.ascontiguousarray(x[:, d]).copy() for d in range(3)]
+    vs = [np.ascontiguousarray(v[:, d]).copy() for d in range(3)]
+    xas = [np.ascontiguousarray(xa[:, d], np.float64) for d in range(3)]
+    mask_all = np.ascontiguousarray(mask_all, np.int32); count = np.ascontiguousarray(count, np.int32)
+    table = np.ascontiguousarray(table, np.int32); types = np.ascontiguousarray(types, np.int32)
+    mt = np.ascontiguousarray(mass_type, np.float64)
+    phi = np.zeros(n)
+    lib().orc_aboundary(n, *[P(a, C.c_double) for a in xs], *[P(a, C.c_double) for a in vs],
+                        *[P(a, C.c_double) for a in xas], P(mask_all, C.c_int32), P(count, C.c_int32),
+                        P(table, C.c_int32), table.shape[1], mobile_bit, wall_bit, C.c_double(cut_phi),
+                        C.c_double(rho_wall), C.c_double(phi_c), C.c_double(0.5 * dt), C.c_double(dt),
+                        P(mt, C.c_double), P(types, C.c_int32), P(phi, C.c_double))
+    return np.stack(xs, 1), np.stack(vs, 1), phi
+
+
 class Sim:
     """The oracle's full single-box engine (the CPU restatement timed as a baseline)."""
 

@@ -41,13 +41,13 @@ timestep 0.01
 run_style mvv/meso
 thermo 100
 """)
-    lam.run(200)
+    lam.run(1000)  # relax the random start (T overshoots, then decays back to kT)
     temps = []
-    for _ in range(16):
-        lam.run(50)
+    for _ in range(20):
+        lam.run(100)
         temps.append(lam.thermo().temp)
     t = lam.thermo()
-    assert abs(np.mean(temps) - 1.0) < 0.02
+    assert abs(np.mean(temps) - 1.0) < 0.01, temps
     assert np.max(np.abs(t.momentum)) < 1e-6 * 3000
     assert "Step Temp" in lam.log
 

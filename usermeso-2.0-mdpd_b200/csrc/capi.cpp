@@ -70,6 +70,8 @@ static void fill_thermo(const Thermo &t, mdpd_thermo_t *o)
     for (int k = 0; k < 6; ++k) o->virial[k] = t.virial[k];
     for (int k = 0; k < 3; ++k) o->momentum[k] = t.mom[k];
     o->temp_group = t.n_group > 1 ? t.ke_group / (3.0 * t.n_group - 3.0) : 0.0;
+    for (int k = 0; k < 6; ++k) o->ptensor[k] = t.ptensor[k];
+    o->surface_tension = t.surface_tension;
     o->status = t.status;
 }
 
@@ -205,7 +207,7 @@ static int64_t field_count(Box &b, const std::string &name)
     if (name == "pos4" || name == "vel4") return 4 * na;
     if (name == "rho") return na;
     if (name == "force") return 4 * n;
-    if (name == "count" || name == "tag" || name == "type" || name == "mask") return n;
+    if (name == "count" || name == "tag" || name == "type" || name == "mask" || name == "phi") return n;
     if (name == "ghost_src" || name == "ghost_img") return st.nghost;
     if (name == "x" || name == "v") return 3 * n;
     if (name == "list") return (int64_t)b.desc.nrow * b.desc.n_col;
@@ -245,6 +247,7 @@ int mdpd_get_field(mdpd_t *h, const char *name, void *out, int64_t nbytes)
         else if (f == "tag") get(B.tag[c], 4);
         else if (f == "type") get(B.type[c], 4);
         else if (f == "mask") get(B.mask[c], 4);
+        else if (f == "phi") get(B.phi[c], 4);
         else if (f == "ghost_src") get(B.gsrc, 4);
         else if (f == "ghost_img") get(B.gimg, 4);
         else if (f == "list") get(B.table, 4);

@@ -536,6 +536,7 @@ void Batch::thermo(std::vector<Thermo> &out)
         t.pe = q[7];
         t.mom[0] = q[8], t.mom[1] = q[9], t.mom[2] = q[10];
         t.ke_group = q[11];
+        for (int k = 0; k < 6; ++k) t.ke_tensor[k] = q[12 + k];
         t.n = bx.n;
         t.n_group = bx.n_group;
         // compute temp (all atoms, dof = 3N - 3) and pressure (compute_pressure_meso.cu:121-150)
@@ -543,6 +544,9 @@ void Batch::thermo(std::vector<Thermo> &out)
         t.temp = dof > 0 ? t.ke_all / dof : 0.0;
         const double vol = bx.desc.prd[0] * bx.desc.prd[1] * bx.desc.prd[2];
         t.press = (dof * t.temp + t.virial[0] + t.virial[1] + t.virial[2]) / 3.0 / vol;
+        // pressure tensor (compute pressure with keyword ke+virial, per component)
+        for (int k = 0; k < 6; ++k) t.ptensor[k] = (t.ke_tensor[k] + t.virial[k]) / vol;
+        t.surface_tension = 0.5 * bx.desc.prd[0] * (t.ptensor[0] - 0.5 * (t.ptensor[1] + t.ptensor[2]));
     }
 }
 

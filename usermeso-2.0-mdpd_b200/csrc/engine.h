@@ -49,7 +49,10 @@ struct Particles {
 struct Thermo {
     long long step = 0, nbuild = 0;
     double ke_all = 0, ke_group = 0, pe = 0, virial[6] = {0, 0, 0, 0, 0, 0}, mom[3] = {0, 0, 0};
+    double ke_tensor[6] = {0, 0, 0, 0, 0, 0};
     double temp = 0, press = 0;
+    double ptensor[6] = {0, 0, 0, 0, 0, 0};  // (kinetic + virial) / V, xx yy zz xy xz yz
+    double surface_tension = 0;              // (Lx/2)(Pxx - (Pyy+Pzz)/2), slab normal to x
     int n = 0, n_group = 0;
     int status = 0;
 };

@@ -428,14 +428,18 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__rest
 }
 
 // ---------------------------------------------------------------------------
-// R11: neighbour list, warp per bin
+// R11: neighbour list, warp per bin.  The 27 stencil bins are concatenated into one
+// candidate stream (lane = candidate, 32 per round); each of up to 32 centres of the bin
+// is tested against the round, hits are inserted by ballot in candidate order, and the
+// centre's running count lives in the register of the lane that owns that centre.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_rb_list(const BoxDesc *__restrict__ boxes,
                                                  const Unit *__restrict__ units, int nunits,
                                                  int nbox, int *done)
 {
-    __shared__ float s_x[8][32], s_y[8][32], s_z[8][32];
-    __shared__ int s_i[8][32], s_n[8][32];
+    __shared__ float4 s_c[8][32];   // centre position, .w = centre index
+    __shared__ int s_base[8][32];   // centre row base in the transposed table
+    __shared__ int s_bs[8][32], s_cum[8][33];
     const int lane = threadIdx.x & 31, w = threadIdx.x / 32;
     const unsigned lt = (1u << lane) - 1u;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
@@ -449,65 +453,74 @@ __global__ void __launch_bounds__(256) k_rb_list(const BoxDesc *__restrict__ box
             const int s = B.bin_start[b], e = B.bin_start[b + 1];
             if (e == s || B.bin_order[s] >= nlocal) continue;  // no locals in this bin
             const int bx = b % B.mbin[0], by = (b / B.mbin[0]) % B.mbin[1], bz = b / (B.mbin[0] * B.mbin[1]);
+            // stencil bins: lane l < 27 takes offset (l%3-1, l/3%3-1, l/9-1)
+            int st = 0, sz = 0;
+            if (lane < 27) {
+                const int x = bx + lane % 3 - 1, y = by + (lane / 3) % 3 - 1, z = bz + lane / 9 - 1;
+                if (x >= 0 && x < B.mbin[0] && y >= 0 && y < B.mbin[1] && z >= 0 && z < B.mbin[2]) {
+                    const int nb = x + B.mbin[0] * (y + z * B.mbin[1]);
+                    st = B.bin_start[nb];
+                    sz = B.bin_start[nb + 1] - st;
+                }
+            }
+            int cum = sz;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, cum, o);
+                if (lane >= o) cum += v;
+            }
+            const int total = __shfl_sync(0xffffffffu, cum, 31);
+            s_bs[w][lane] = st;
+            s_cum[w][lane + 1] = cum;
+            if (lane == 0) s_cum[w][0] = 0;
+            __syncwarp();
             for (int cb = s; cb < e; cb += 32) {
-                // centre batch: members with index < nlocal (they come first)
+                // centre batch: members with index < nlocal (they come first in a bin)
                 const int pc = cb + lane;
-                int ci = pc < e ? B.bin_order[pc] : nlocal;
+                const int ci = pc < e ? B.bin_order[pc] : nlocal;
                 const bool is_c = ci < nlocal;
                 const unsigned cm = __ballot_sync(0xffffffffu, is_c);
                 if (cm == 0) break;
                 const int nc = __popc(cm);
                 if (is_c) {
-                    const float4 p = B.bpos[pc];
-                    s_x[w][lane] = p.x, s_y[w][lane] = p.y, s_z[w][lane] = p.z;
-                    s_i[w][lane] = ci;
-                    s_n[w][lane] = 0;
+                    float4 p = B.bpos[pc];
+                    p.w = __int_as_float(ci);
+                    s_c[w][lane] = p;
+                    s_base[w][lane] = (ci & ~31) * ncol + (ci & 31);
                 }
+                int my_n = 0;  // running count of the centre owned by this lane
                 __syncwarp();
-                for (int dz = -1; dz <= 1; ++dz) {
-                    const int z = bz + dz;
-                    if (z < 0 || z >= B.mbin[2]) continue;
-                    for (int dy = -1; dy <= 1; ++dy) {
-                        const int y = by + dy;
-                        if (y < 0 || y >= B.mbin[1]) continue;
-                        for (int dx = -1; dx <= 1; ++dx) {
-                            const int x = bx + dx;
-                            if (x < 0 || x >= B.mbin[0]) continue;
-                            const int nb = x + B.mbin[0] * (y + z * B.mbin[1]);
-                            const int ps = B.bin_start[nb], pe = B.bin_start[nb + 1];
-                            for (int p0 = ps; p0 < pe; p0 += 32) {
-                                const int p = p0 + lane;
-                                const bool valid = p < pe;
-                                float4 pj = make_float4(1e30f, 1e30f, 1e30f, 0.f);
-                                int j = -1;
-                                if (valid) {
-                                    pj = B.bpos[p];
-                                    j = B.bin_order[p];
-                                }
-                                for (int q = 0; q < nc; ++q) {
-                                    const float ddx = s_x[w][q] - pj.x, ddy = s_y[w][q] - pj.y,
-                                                ddz = s_z[w][q] - pj.z;
-                                    const float r2 = dist2(ddx, ddy, ddz);
-                                    const int cq = s_i[w][q];
-                                    const bool hit = valid && r2 <= rc2 && j != cq;
-                                    const unsigned bal = __ballot_sync(0xffffffffu, hit);
-                                    if (bal) {
-                                        const int kq = s_n[w][q] + __popc(bal & lt);
-                                        if (hit && kq < ncol) B.table[list_addr(cq, kq, ncol)] = j;
-                                        __syncwarp();
-                                        if (lane == 0) s_n[w][q] += __popc(bal);
-                                        __syncwarp();
-                                    }
-                                }
-                            }
+                for (int q0 = 0; q0 < total; q0 += 32) {
+                    const int q = q0 + lane;
+                    const bool valid = q < total;
+                    float4 pj = make_float4(1e30f, 1e30f, 1e30f, 0.f);
+                    int j = -1;
+                    if (valid) {
+                        int lo = 0, hi = 27;  // largest slot with s_cum[slot] <= q
+                        while (hi - lo > 1) {
+                            const int mid = (lo + hi) >> 1;
+                            if (s_cum[w][mid] <= q) lo = mid;
+                            else hi = mid;
+                        }
+                        const int p = s_bs[w][lo] + (q - s_cum[w][lo]);
+                        pj = B.bpos[p];
+                        j = B.bin_order[p];
+                    }
+                    for (int c = 0; c < nc; ++c) {
+                        const float4 cc = s_c[w][c];
+                        const float r2 = dist2(cc.x - pj.x, cc.y - pj.y, cc.z - pj.z);
+                        const bool hit = r2 <= rc2 && j != __float_as_int(cc.w) && valid;
+                        const unsigned bal = __ballot_sync(0xffffffffu, hit);
+                        if (bal) {
+                            const int kq = __shfl_sync(0xffffffffu, my_n, c) + __popc(bal & lt);
+                            if (hit && kq < ncol) B.table[s_base[w][c] + (kq & 31) * ncol + (kq & ~31)] = j;
+                            if (lane == c) my_n += __popc(bal);
                         }
                     }
                 }
                 if (is_c) {
-                    const int n = s_n[w][lane];
-                    B.count[ci] = n < ncol ? n : ncol;
-                    if (n > ncol) atomicOr(&B.st->status, kErrListOverflow);
-                    local_max = max(local_max, n);
+                    B.count[ci] = my_n < ncol ? my_n : ncol;
+                    if (my_n > ncol) atomicOr(&B.st->status, kErrListOverflow);
+                    local_max = max(local_max, my_n);
                 }
                 __syncwarp();
             }

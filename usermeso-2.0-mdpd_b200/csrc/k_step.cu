@@ -212,15 +212,27 @@ __global__ void __launch_bounds__(kUnit *TPP) k_density(const BoxDesc *__restric
             const float4 pi = B.pos[i];
             const float h = B.cut_rho, h2 = h * h;
             const int n = B.count[i];
-            const int *row = B.table + (i & ~31) * B.n_col + (i & 31);
-            for (int k = t; k < n; k += TPP) {
-                const int j = __ldg(row + (k & 31) * B.n_col + (k & ~31));
-                const float4 pj = __ldg(&B.pos[j]);
-                const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                const float rsq = dist2(dx, dy, dz);
-                if (rsq < h2 && rsq >= 1e-20f) {
-                    const float d = h - sqrtf(rsq);
-                    acc = __fmaf_rn(d, d, acc);
+            const int ncol = B.n_col;
+            const int *row = B.table + (i & ~31) * ncol + (i & 31);
+            // four independent index -> position gather chains in flight per thread
+            for (int k0 = t; k0 < n; k0 += 4 * TPP) {
+                int j[4];
+                float4 pj[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int k = k0 + q * TPP;
+                    j[q] = k < n ? __ldcs(row + (k & 31) * ncol + (k & ~31)) : -1;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) pj[q] = j[q] >= 0 ? __ldg(&B.pos[j[q]]) : make_float4(1e30f, 0, 0, 0);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float dx = pi.x - pj[q].x, dy = pi.y - pj[q].y, dz = pi.z - pj[q].z;
+                    const float rsq = dist2(dx, dy, dz);
+                    if (rsq < h2 && rsq >= 1e-20f) {
+                        const float d = h - sqrtf(rsq);
+                        acc = __fmaf_rn(d, d, acc);
+                    }
                 }
             }
         }
@@ -252,6 +264,8 @@ void launch_density(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const S
 // it, the conservative + dissipative + random force with the pairwise gaussian of the
 // two signatures.  Epilogue (t==0): + body force, store f, final half-kick (FP64 v).
 // ---------------------------------------------------------------------------
+constexpr int kQueue = 16;  // list entries tested per phase-1 round of the force pass
+
 struct EvAcc {
     float vxx, vyy, vzz, vxy, vxz, vyz, pe;
 };
@@ -262,6 +276,7 @@ __global__ void __launch_bounds__(kUnit *TPP) k_force(const BoxDesc *__restrict_
 {
     __shared__ PairCoeff s_coeff[kMaxTypes * kMaxTypes];
     __shared__ double s_red[kUnit * TPP / 32][7];
+    __shared__ int s_q[kQueue][kUnit * TPP];  // per-thread queue of in-range neighbours
     int cur_box = -1;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const Unit U = units[u];
@@ -300,14 +315,39 @@ __global__ void __launch_bounds__(kUnit *TPP) k_force(const BoxDesc *__restrict_
             }
             const float dtis = B.dt_inv_sqrt;
             const int n = B.count[i];
-            const int *row = B.table + (i & ~31) * B.n_col + (i & 31);
-            for (int k = t; k < n; k += TPP) {
-                const int j = __ldg(row + (k & 31) * B.n_col + (k & ~31));
-                const float4 pj = __ldg(&B.pos[j]);
-                const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                const float rsq = dist2(dx, dy, dz);
-                const PairCoeff &cf = s_coeff[ti * ntype + ptype(pj)];
-                if (rsq < cf.cutsq && rsq >= 1e-20f) {
+            const int ncol = B.n_col;
+            const int *row = B.table + (i & ~31) * ncol + (i & 31);
+            for (int kb = t; kb < n; kb += kQueue * TPP) {
+                // phase 1: distance test of up to kQueue entries, four gathers in flight;
+                // in-range neighbours are queued (this thread's column of s_q)
+                int nq = 0;
+#pragma unroll
+                for (int b4 = 0; b4 < kQueue; b4 += 4) {
+                    int j[4];
+                    float4 pj[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int k = kb + (b4 + q) * TPP;
+                        j[q] = k < n ? __ldcs(row + (k & 31) * ncol + (k & ~31)) : -1;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        pj[q] = j[q] >= 0 ? __ldg(&B.pos[j[q]]) : make_float4(1e30f, 0, 0, 0);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float dx = pi.x - pj[q].x, dy = pi.y - pj[q].y, dz = pi.z - pj[q].z;
+                        const float rsq = dist2(dx, dy, dz);
+                        if (j[q] >= 0 && rsq < s_coeff[ti * ntype + ptype(pj[q])].cutsq && rsq >= 1e-20f)
+                            s_q[nq++][threadIdx.x] = j[q];
+                    }
+                }
+                // phase 2: forces of the queued neighbours, in list order
+                for (int q = 0; q < nq; ++q) {
+                    const int j = s_q[q][threadIdx.x];
+                    const float4 pj = __ldg(&B.pos[j]);
+                    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                    const float rsq = dist2(dx, dy, dz);
+                    const PairCoeff &cf = s_coeff[ti * ntype + ptype(pj)];
                     const float4 vj = __ldg(&B.vel[j]);
                     const float rinv = rsqrtf(rsq);
                     const float r = rsq * rinv;
@@ -450,38 +490,43 @@ void launch_force(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const Ste
 
 // ---------------------------------------------------------------------------
 // thermo: per-unit kinetic energy / momentum partials, then per-box sums in unit order.
-// out[box*kPartialStride + q]: q=0 sum m v^2 (all), 1..6 virial, 7 pe, 8..10 momentum,
-// 11 sum m v^2 over the nve group.
+// slots: 0 sum m v^2 (all), 1..6 virial xx yy zz xy xz yz (force pass), 7 pair energy,
+// 8..10 momentum, 11 sum m v^2 over the nve group, 12..17 kinetic tensor xx yy zz xy xz yz.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kUnit) k_thermo_units(const BoxDesc *__restrict__ boxes,
                                                         const Unit *__restrict__ units, int nunits)
 {
-    __shared__ double s_red[kUnit / 32][5];
+    constexpr int NQ = 11;
+    __shared__ double s_red[kUnit / 32][NQ];
+    const int slot[NQ] = {0, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17};
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const Unit U = units[u];
         const BoxDesc &B = boxes[U.box];
         const int c = B.st->cur;
         const int i = U.begin + threadIdx.x;
-        double vals[5] = {0, 0, 0, 0, 0};
+        double vals[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) vals[q] = 0.0;
         if (i < U.end) {
             const int t = B.type[c][i];
             const double m = B.mass[t - 1];
             const double vx = B.v[c][0][i], vy = B.v[c][1][i], vz = B.v[c][2][i];
             vals[0] = m * (vx * vx + vy * vy + vz * vz);
-            if (B.mask[c][i] & B.nve_bit) vals[4] = vals[0];
             vals[1] = m * vx, vals[2] = m * vy, vals[3] = m * vz;
+            if (B.mask[c][i] & B.nve_bit) vals[4] = vals[0];
+            vals[5] = m * vx * vx, vals[6] = m * vy * vy, vals[7] = m * vz * vz;
+            vals[8] = m * vx * vy, vals[9] = m * vx * vz, vals[10] = m * vy * vz;
         }
 #pragma unroll
-        for (int q = 0; q < 5; ++q)
+        for (int q = 0; q < NQ; ++q)
             for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_down_sync(0xffffffffu, vals[q], o);
         if ((threadIdx.x & 31) == 0)
-            for (int q = 0; q < 5; ++q) s_red[threadIdx.x / 32][q] = vals[q];
+            for (int q = 0; q < NQ; ++q) s_red[threadIdx.x / 32][q] = vals[q];
         __syncthreads();
-        if (threadIdx.x < 5) {
+        if (threadIdx.x < NQ) {
             double a = 0.0;
             for (int w = 0; w < kUnit / 32; ++w) a += s_red[w][threadIdx.x];
-            const int slot = threadIdx.x == 0 ? 0 : 7 + threadIdx.x;  // ke_all, px, py, pz, ke_group
-            B.partial[(size_t)(U.begin / kUnit) * kPartialStride + slot] = a;
+            B.partial[(size_t)(U.begin / kUnit) * kPartialStride + slot[threadIdx.x]] = a;
         }
         __syncthreads();
     }

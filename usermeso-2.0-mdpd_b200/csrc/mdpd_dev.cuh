@@ -103,11 +103,11 @@ struct BoxDesc {
     float4 *bpos;         // positions in bin order
     int *scan_part;       // per-chunk partial sums for scans
     // ---- thermo partials ----
-    double *partial;      // per unit: [ke, vir_xx, vir_yy, vir_zz, vir_xy, vir_xz, vir_yz, pe, px, py, pz]
+    double *partial;      // per unit thermo partials (kPartialStride doubles)
     BoxState *st;
 };
 
-constexpr int kPartialStride = 12;
+constexpr int kPartialStride = 18;  // see k_thermo_units for the slot map
 
 // ---------------------------------------------------------------------------
 // counter-based RNG (TEA, GPU variant of Zafar et al.) and the reference's

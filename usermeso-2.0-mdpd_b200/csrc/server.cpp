@@ -203,6 +203,9 @@ void mdpd_server_s::loop()
                 out.press = t.press;
                 out.ke = 0.5 * t.ke_all;
                 for (int d = 0; d < 3; ++d) out.momentum[d] = t.mom[d];
+                for (int d = 0; d < 6; ++d) out.ptensor[d] = t.ptensor[d];
+                out.pe = t.pe;
+                out.surface_tension = t.surface_tension;
                 out.status = t.status;
                 std::vector<double> xf, vf;
                 if (j->spec.keep_state && !fail) {

@@ -31,6 +31,7 @@ class Thermo(C.Structure):
     _fields_ = [("step", C.c_int64), ("natoms", C.c_int64), ("nbuild", C.c_int64),
                 ("temp", C.c_double), ("press", C.c_double), ("pe", C.c_double), ("ke", C.c_double),
                 ("virial", C.c_double * 6), ("momentum", C.c_double * 3), ("temp_group", C.c_double),
+                ("ptensor", C.c_double * 6), ("surface_tension", C.c_double),
                 ("status", C.c_int32), ("pad", C.c_int32)]
 
 
@@ -176,7 +177,7 @@ class Lammps:
     def field(self, name):
         n = C.c_int64()
         self._check(lib().mdpd_field_size(self.h, name.encode(), C.byref(n)))
-        dt = {"pos4": np.float32, "vel4": np.float32, "rho": np.float32, "force": np.float32,
+        dt = {"pos4": np.float32, "vel4": np.float32, "rho": np.float32, "force": np.float32, "phi": np.float32,
               "x": np.float64, "v": np.float64}.get(name, np.int32)
         out = np.zeros(max(n.value, 1), dt)
         self._check(lib().mdpd_get_field(self.h, name.encode(), out.ctypes.data_as(C.c_void_p), out.nbytes))
