@@ -518,7 +518,7 @@ int orc_build_list(const orc_box *b, int nlocal, int nall, const double *x, cons
 /* pair passes                                                           */
 /* ===================================================================== */
 
-static int type_of(const float *pos4, int i) { return (int)f2u(pos4[4 * i + 3]); }
+static int type_of(const float *pos4, int i) { return (int)(f2u(pos4[4 * i + 3]) & 0xFFu); /* low byte: type-1 */ }
 
 void orc_density(int nlocal, const float *pos4, const int32_t *count, const int32_t *table,
                  int n_col, const int32_t *mask, int groupbit, double cut_rho,

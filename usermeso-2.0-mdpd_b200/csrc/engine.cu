@@ -28,8 +28,8 @@ static int ceil_to(int x, int inc) { return ((x + inc - 1) / inc) * inc; }
 
 struct Geometry {
     double prd[3], cen[3], cutneighmax, cutghost, binsize[3], bininv[3];
-    int mbin[3], n_col;
-    float rc2_tail;
+    int mbin[3], n_col, n_col2;
+    float rc2_tail, rc2_force;
 };
 
 static Geometry geometry(const Spec &s, int n)
@@ -59,6 +59,10 @@ static Geometry geometry(const Spec &s, int n)
         g.bininv[d] = 1.0 / g.binsize[d];
     }
     g.rc2_tail = (float)std::pow(g.cutneighmax, 2.0);
+    double e2 = dens * (4.0 / 3.0 * 3.142 * std::pow(cutforce, 3.0)) * 4.0 * 0.5;  // half list
+    e2 = std::max(e2, 32.0);
+    g.n_col2 = ceil_to((int)e2, 32);
+    g.rc2_force = (float)(cutforce * cutforce);
     return g;
 }
 
@@ -81,6 +85,7 @@ size_t Box::estimate_bytes(const Spec &spec, int n)
     b += (size_t)(n + gc) * (16 + 16 + 4 + 4 + 4 + 16 + 4);                      // pos, vel, rho, bin_of, bin_order, bpos, gfirst
     b += (size_t)gc * 8;
     b += (size_t)nrow * g.n_col * 4;
+    if (spec.style == 0) b += (size_t)nrow * (g.n_col2 + 1) * 4 + (size_t)n * 24;
     b += (size_t)nbin * (4 + 3 * 4) * 3;
     b += (size_t)((n + kUnit - 1) / kUnit) * kPartialStride * 8;
     return b + (1u << 20);
@@ -129,6 +134,8 @@ Box::Box(const Spec &s, const Particles &p, int sms) : spec(s)
     B.cutghost = g.cutghost;
     B.triggersq = 0.25 * s.skin * s.skin;
     B.rc2_tail = g.rc2_tail;
+    B.rc2_force = g.rc2_force;
+    B.n_col2 = g.n_col2;
     nbin = B.nbin = g.mbin[0] * g.mbin[1] * g.mbin[2];
     B.nlocal = n;
     B.nrow = ceil_to(n, 32);
@@ -206,6 +213,11 @@ Box::Box(const Spec &s, const Particles &p, int sms) : spec(s)
     B.gfirst = alloc<int>(n + 1);
     B.count = alloc<int>(B.nrow);
     B.table = alloc<int>((size_t)B.nrow * B.n_col);
+    if (s.style == 0) {
+        B.count2 = alloc<int>(B.nrow);
+        B.table2 = alloc<int>((size_t)B.nrow * B.n_col2);
+        B.facc = alloc<unsigned long long>(3 * (size_t)n);
+    }
     B.bin_rank = alloc<int>(nbin);
     B.cls_count = alloc<int>(2 * (size_t)nbin + 1);
     B.cls_start = alloc<int>(2 * (size_t)nbin + 1);
@@ -320,6 +332,9 @@ void Box::upload_xv(const double *x, const double *v)
 Batch::Batch(std::vector<Box *> boxes, const StepConfig &c) : cfg(c), boxes_(std::move(boxes))
 {
     if (boxes_.empty()) throw std::runtime_error("ARG: empty batch");
+    cfg.uniform_types = 1;
+    for (Box *b : boxes_) cfg.uniform_types &= b->desc.ntype == 1;
+    cfg.half = cfg.style == 0 && !cfg.wall_coupling && cfg.half_enabled;
     check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
     const int nb = (int)boxes_.size();
     check_cuda(cudaMalloc(&d_boxes, sizeof(BoxDesc) * nb), "boxes");
@@ -465,7 +480,10 @@ void Batch::reconfigure(const StepConfig &c)
         graph_[k] = nullptr;
         graph_src_[k] = nullptr;
     }
+    const int uni = cfg.uniform_types, half = cfg.half;
     cfg = c;
+    cfg.uniform_types = uni;
+    cfg.half = half;
     capture(0);
     capture(1);
 }

@@ -12,6 +12,7 @@
 //   force (dpd)    pair_dpd_meso.cu:91-205
 //   rebuild check  neighbor.cpp:1216-1231 (decide), :1244-1322 (check_distance)
 #include "kernels.h"
+#include "pair.cuh"
 
 #include <cstdio>
 
@@ -196,7 +197,7 @@ void launch_force_rebuild_flag(cudaStream_t s, BoxDesc *boxes, int nbox, int val
 // TPP threads per particle split the list and combine with shuffles.
 // ---------------------------------------------------------------------------
 template <int TPP>
-__global__ void __launch_bounds__(kUnit *TPP) k_density(const BoxDesc *__restrict__ boxes,
+__global__ void __launch_bounds__(kUnit *TPP, 16 / TPP) k_density(const BoxDesc *__restrict__ boxes,
                                                          const Unit *__restrict__ units, int nunits)
 {
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
@@ -227,12 +228,11 @@ __global__ void __launch_bounds__(kUnit *TPP) k_density(const BoxDesc *__restric
                 for (int q = 0; q < 4; ++q) pj[q] = j[q] >= 0 ? __ldg(&B.pos[j[q]]) : make_float4(1e30f, 0, 0, 0);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
+                    // branchless: (h - r)^2 for 1e-20 <= r^2 < h^2, else 0
                     const float dx = pi.x - pj[q].x, dy = pi.y - pj[q].y, dz = pi.z - pj[q].z;
                     const float rsq = dist2(dx, dy, dz);
-                    if (rsq < h2 && rsq >= 1e-20f) {
-                        const float d = h - sqrtf(rsq);
-                        acc = __fmaf_rn(d, d, acc);
-                    }
+                    const float d = (rsq < h2 && rsq >= 1e-20f) ? h - rsq * rsqrtf(rsq) : 0.f;
+                    acc = __fmaf_rn(d, d, acc);
                 }
             }
         }
@@ -252,6 +252,10 @@ __global__ void __launch_bounds__(kUnit *TPP) k_density(const BoxDesc *__restric
 void launch_density(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c)
 {
     const int grid = u.local.n < c.sms * 16 ? (u.local.n > 0 ? u.local.n : 1) : c.sms * 16;
+    if (c.half) {
+        launch_density_half(s, boxes, u, c);
+        return;
+    }
     switch (c.tpp_density) {
     case 2: k_density<2><<<grid, kUnit * 2, 0, s>>>(boxes, u.local.d, u.local.n); break;
     case 4: k_density<4><<<grid, kUnit * 4, 0, s>>>(boxes, u.local.d, u.local.n); break;
@@ -266,12 +270,8 @@ void launch_density(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const S
 // ---------------------------------------------------------------------------
 constexpr int kQueue = 16;  // list entries tested per phase-1 round of the force pass
 
-struct EvAcc {
-    float vxx, vyy, vzz, vxy, vxz, vyz, pe;
-};
-
-template <int TPP, int STYLE, bool EXACT, bool EV, bool WALLC>
-__global__ void __launch_bounds__(kUnit *TPP) k_force(const BoxDesc *__restrict__ boxes,
+template <int TPP, int STYLE, bool EXACT, bool EV, bool WALLC, bool UNI>
+__global__ void __launch_bounds__(kUnit *TPP, 10 / TPP) k_force(const BoxDesc *__restrict__ boxes,
                                                        const Unit *__restrict__ units, int nunits, int kick)
 {
     __shared__ PairCoeff s_coeff[kMaxTypes * kMaxTypes];
@@ -337,7 +337,8 @@ __global__ void __launch_bounds__(kUnit *TPP) k_force(const BoxDesc *__restrict_
                     for (int q = 0; q < 4; ++q) {
                         const float dx = pi.x - pj[q].x, dy = pi.y - pj[q].y, dz = pi.z - pj[q].z;
                         const float rsq = dist2(dx, dy, dz);
-                        if (j[q] >= 0 && rsq < s_coeff[ti * ntype + ptype(pj[q])].cutsq && rsq >= 1e-20f)
+                        const int cid = UNI ? 0 : ti * ntype + ptype(pj[q]);
+                        if (j[q] >= 0 && rsq < s_coeff[cid].cutsq && rsq >= 1e-20f)
                             s_q[nq++][threadIdx.x] = j[q];
                     }
                 }
@@ -345,50 +346,8 @@ __global__ void __launch_bounds__(kUnit *TPP) k_force(const BoxDesc *__restrict_
                 for (int q = 0; q < nq; ++q) {
                     const int j = s_q[q][threadIdx.x];
                     const float4 pj = __ldg(&B.pos[j]);
-                    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                    const float rsq = dist2(dx, dy, dz);
-                    const PairCoeff &cf = s_coeff[ti * ntype + ptype(pj)];
-                    const float4 vj = __ldg(&B.vel[j]);
-                    const float rinv = rsqrtf(rsq);
-                    const float r = rsq * rinv;
-                    if (r < 1e-10f) continue;
-                    const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
-                    const float dot = __fmaf_rn(dz, dvz, __fmaf_rn(dy, dvy, dx * dvx));
-                    const float wc = 1.f - r * cf.inv_cut;
-                    float gam = cf.gamma, sig = cf.sigma;
-                    float rn;
-                    if (EXACT)
-                        rn = (float)gaussian_exact(si, __float_as_uint(vj.w));
-                    else
-                        rn = gaussian_fast(si, __float_as_uint(vj.w));
-                    float fpair;
-                    if (STYLE == 0) {
-                        const float wcr = fmaxf(1.f - r * cf.inv_cut_r, 0.f);
-                        const float rho_j = __ldg(&B.rho[j]);
-                        if (WALLC && i_mobile && (pflags(pj) & 2)) {
-                            sig *= wall_sqrt;
-                            gam *= wall_ratio;
-                        }
-                        fpair = (cf.A * wc + cf.B * (rho_i + rho_j) * wcr) - gam * wc * wc * dot * rinv +
-                                sig * wc * rn * dtis;
-                        if (EV) ev.pe += cf.e_cut * wc * wc + cf.e_cut_r * (rho_i + rho_j) * wcr * wcr;
-                    } else {
-                        const float wr = cf.expw == 1.f ? wc : __powf(wc, cf.expw);
-                        fpair = cf.A * wc - gam * wr * wr * dot * rinv + sig * wr * rn * dtis;
-                        if (EV) ev.pe += cf.e_cut * wc * wc;
-                    }
-                    fpair *= rinv;
-                    fx = __fmaf_rn(dx, fpair, fx);
-                    fy = __fmaf_rn(dy, fpair, fy);
-                    fz = __fmaf_rn(dz, fpair, fz);
-                    if (EV) {
-                        ev.vxx += dx * dx * fpair;
-                        ev.vyy += dy * dy * fpair;
-                        ev.vzz += dz * dz * fpair;
-                        ev.vxy += dx * dy * fpair;
-                        ev.vxz += dx * dz * fpair;
-                        ev.vyz += dy * dz * fpair;
-                    }
+                    pair_term<STYLE, EXACT, EV, WALLC>(B, s_coeff[UNI ? 0 : ti * ntype + ptype(pj)], j, pj, pi, vi, si,
+                                                       rho_i, i_mobile, wall_ratio, wall_sqrt, dtis, fx, fy, fz, ev);
                 }
             }
         }
@@ -449,12 +408,15 @@ __global__ void __launch_bounds__(kUnit *TPP) k_force(const BoxDesc *__restrict_
 }
 
 template <int TPP, int STYLE, bool EXACT, bool EV>
-static void force_launch_wall(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, int grid, int wallc, int kick)
+static void force_launch_wall(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, int grid, int wallc, int kick,
+                              int uniform)
 {
     if (wallc)
-        k_force<TPP, STYLE, EXACT, EV, true><<<grid, kUnit * TPP, 0, s>>>(boxes, u.local.d, u.local.n, kick);
+        k_force<TPP, STYLE, EXACT, EV, true, false><<<grid, kUnit * TPP, 0, s>>>(boxes, u.local.d, u.local.n, kick);
+    else if (uniform)
+        k_force<TPP, STYLE, EXACT, EV, false, true><<<grid, kUnit * TPP, 0, s>>>(boxes, u.local.d, u.local.n, kick);
     else
-        k_force<TPP, STYLE, EXACT, EV, false><<<grid, kUnit * TPP, 0, s>>>(boxes, u.local.d, u.local.n, kick);
+        k_force<TPP, STYLE, EXACT, EV, false, false><<<grid, kUnit * TPP, 0, s>>>(boxes, u.local.d, u.local.n, kick);
 }
 
 template <int TPP, int STYLE>
@@ -462,11 +424,11 @@ static void force_launch_tpp(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u
                              const StepConfig &c, int ev, int kick)
 {
     if (c.exact_rng) {
-        if (ev) force_launch_wall<TPP, STYLE, true, true>(s, boxes, u, grid, c.wall_coupling, kick);
-        else force_launch_wall<TPP, STYLE, true, false>(s, boxes, u, grid, c.wall_coupling, kick);
+        if (ev) force_launch_wall<TPP, STYLE, true, true>(s, boxes, u, grid, c.wall_coupling, kick, c.uniform_types);
+        else force_launch_wall<TPP, STYLE, true, false>(s, boxes, u, grid, c.wall_coupling, kick, c.uniform_types);
     } else {
-        if (ev) force_launch_wall<TPP, STYLE, false, true>(s, boxes, u, grid, c.wall_coupling, kick);
-        else force_launch_wall<TPP, STYLE, false, false>(s, boxes, u, grid, c.wall_coupling, kick);
+        if (ev) force_launch_wall<TPP, STYLE, false, true>(s, boxes, u, grid, c.wall_coupling, kick, c.uniform_types);
+        else force_launch_wall<TPP, STYLE, false, false>(s, boxes, u, grid, c.wall_coupling, kick, c.uniform_types);
     }
 }
 
@@ -483,6 +445,10 @@ static void force_launch_style(cudaStream_t s, BoxDesc *boxes, const BatchUnits 
 
 void launch_force(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev, int kick)
 {
+    if (c.half) {
+        launch_force_half(s, boxes, u, c, ev, kick);
+        return;
+    }
     const int grid = u.local.n < c.sms * 16 ? (u.local.n > 0 ? u.local.n : 1) : c.sms * 16;
     if (c.style == 0) force_launch_style<0>(s, boxes, u, grid, c, ev, kick);
     else force_launch_style<1>(s, boxes, u, grid, c, ev, kick);

@@ -32,6 +32,9 @@ struct StepConfig {
     int wall = 0;          // aboundary bounce-back in the integrate pass
     int wall_coupling = 0; // phi-dependent gamma/sigma in the force pass
     int style = 0;         // 0 mdpd, 1 dpd
+    int uniform_types = 0; // every box has one atom type: constant coefficient index
+    int half = 0;          // mdpd without wall coupling: each pair evaluated once (k_pair.cu)
+    int half_enabled = 1;  // allow the half-list passes (set per batch from the boxes)
     int sms = 148;
 };
 
@@ -49,6 +52,8 @@ void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const S
 void launch_density(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c);
 void launch_force(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev,
                   int kick);
+void launch_density_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c);
+void launch_force_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev, int kick);
 void launch_thermo(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, double *out, int *done);
 void launch_density_profile(cudaStream_t s, const BoxDesc *boxes, int box, const Unit *units,
                             int nunits, int dim, int groupbit, double lo, double inv, int nbin,

@@ -22,6 +22,7 @@ enum : int {
     kErrBucketOverflow = 4, // a bin or reorder bucket holds more than kClassMax particles
     kErrNonFinite = 8,      // NaN/Inf force
     kErrLost = 16,          // particle outside the box by more than one period
+    kErrList2Overflow = 32, // more force-range neighbours than the compact list holds
 };
 
 struct PairCoeff {  // per type pair; FP32 pair arithmetic
@@ -91,6 +92,12 @@ struct BoxDesc {
     int *gsrc, *gimg, *gfirst;
     // ---- neighbour list (locally transposed: 32-row blocks) ----
     int *count, *table;
+    // entries within the force cutoff whose source index is above the particle's (each pair
+    // once), compacted by the density pass for the force pass
+    int *count2, *table2;
+    int n_col2;
+    unsigned long long *facc;  // 3 x nlocal fixed-point force sums (2^-32 units), SoA
+    float rc2_force;      // largest force cutoff squared
     // ---- rebuild scratch ----
     int *bin_rank;        // Morton rank of each bin (reorder class order)
     int *cls_count, *cls_start, *cls_cursor;  // 2*nbin
@@ -272,10 +279,12 @@ __device__ __forceinline__ float gaussian_fast(uint32_t si, uint32_t sj)
     s = __fmaf_rn(s, x2, -1.57079632662144460E+0f);
     const float f = (v0 & 0x80000000u) ? s * x : -s * x;
     const uint32_t w = max(v1, 1u);
-    // log2(w * 2^-32): log1p of the (exact) distance to 2^32 in the upper half
+    // log2(w * 2^-32): log1p of the exact distance to 2^32 in the upper half (small |L|, where
+    // relative accuracy matters); the hardware log2 below 2^31, where |L| >= 1
     const float l = w >= 0x80000000u ? log1pf(-(float)(0u - w) * 2.3283064365386963e-10f) * 1.4426950408889634f
-                                     : log2f((float)w) - 32.0f;
-    const float r = sqrtf(fmaxf((float)(-2.0 * 6.9314718055994528623E-1) * l, 0.0f));
+                                     : __log2f((float)w) - 32.0f;
+    const float a = (float)(-2.0 * 6.9314718055994528623E-1) * l;  // > 0: w <= 2^32 - 1
+    const float r = a * rsqrtf(a);
     return fmaxf(-4.0f, fminf(r * f, 4.0f));
 }
 
