@@ -172,6 +172,32 @@ int mdpd_server_drain(mdpd_server_t *s, double timeout_s);
 int mdpd_server_stats(mdpd_server_t *s, double *out7);
 void mdpd_server_stop(mdpd_server_t *s);
 
+/* --- kinetic sums over caller-owned device arrays, allocating nothing -------------------
+ * No counterpart in the reference. For callers that own all the device memory they want used
+ * and call in from inside their own timestep (a LAMMPS fix/compute on its USER-MESO device
+ * arrays, an application whose caching allocator or fixed arena holds the GPU): they cannot
+ * let the library allocate, because cudaMalloc/cudaFree synchronise the whole device and fail
+ * when the caller's pool holds the memory. This call uses no cudaMalloc, cudaFree or other
+ * allocating routine; its scratch is a fixed 1.44 MB device array that every GPU loading the
+ * library holds until the process exits.
+ *   vx, vy, vz, mass: n doubles each, device memory of the current device (per-particle
+ *   velocity components and mass, the layout of MesoAtomVec's dev_veloc(0..2) and dev_mass);
+ *   mask: n ints on the device, or NULL to count every particle; a particle is counted when
+ *   mask[i] & groupbit. stream: a cudaStream_t (NULL = the legacy default stream); the call
+ *   returns after that stream has finished its work.
+ *   sums (host, 11 doubles): sum m v^2, sum m v (x, y, z), sum m v_a v_b (xx yy zz xy xz yz),
+ *   number of particles counted. Temperature in lj units is sums[0] / (3 sums[10] - 3).
+ *   err (optional, err_len bytes): the reason for a non-zero return.
+ * Limit: n <= 16,777,216 (2^24) per call; larger n returns MDPD_ERR_ARG without launching.
+ * The first call on each device looks up the scratch array's device address with that
+ * device current; make that first call before any stream capture. Every call on a device
+ * shares the one scratch array: calls whose work overlaps on the GPU (two host threads on two
+ * streams, say) race and can return wrong sums, so run them one after another. Nothing needs
+ * clearing between calls: each call writes every scratch entry it reads. */
+int mdpd_kinetic_sums_noalloc(const double *vx, const double *vy, const double *vz,
+                              const double *mass, const int32_t *mask, int32_t groupbit,
+                              int64_t n, void *stream, double *sums, char *err, int64_t err_len);
+
 #ifdef __cplusplus
 }
 #endif
