@@ -1,178 +1,220 @@
 // mDPD pair passes with each pair evaluated once.
 //
-// k_density_staged: per warp of 32 consecutive particles, the list window of every lane is
-//   loaded with all its loads in flight into shared memory (coalesced, locally transposed
-//   table), then each lane gathers its neighbours' positions eight at a time.  It computes
-//   rho_i (fix_aboundary_rho_meso.cu:119-165) and appends to a second, compact table the
-//   entries j within the force cutoff whose source particle is above i, so every pair
-//   appears once.
-// k_force_half: for each compact entry, the mDPD pair force (pair_mdpd_meso.cu:139-225) is
-//   evaluated once; +F goes to i and -F to j through 64-bit fixed-point sums (2^-32 units).
-//   Integer addition is associative, so the sums do not depend on the order of the atomics:
-//   results are bitwise reproducible, and the pairwise forces cancel exactly (momentum).
+// k_density_rows: one lane per particle row of the full list (32 consecutive particles per
+//   warp, the locally transposed table makes each entry index a coalesced warp load), eight
+//   neighbour positions in flight per lane. It computes rho_i (fix_aboundary_rho_meso.cu:
+//   119-165) and writes, into the particle's row of the compact table, the entries within the
+//   force cutoff that the row owns: a local j when j > i, a ghost j when j is an image shifted
+//   in the positive direction (kUpperImage in pos.w). The mirrored pair, seen from the other
+//   end, has the opposite shift, so every pair is owned by exactly one row.
+// k_force_pairs: the 32 compact rows of a warp are concatenated and split into 32 equal
+//   contiguous shares, one per lane (a prefix scan of the row lengths and one binary search),
+//   so every lane evaluates the same number of pairs whatever the row lengths. The mDPD pair
+//   force (pair_mdpd_meso.cu:139-225) is summed for the row in 64-bit fixed point (2^-32
+//   units) in registers and flushed when the lane's share moves to the next row; -F goes to
+//   j's source particle in the same fixed point, through shared memory when the source is
+//   one of the block's 128 rows and global 64-bit atomics otherwise. Integer addition is
+//   associative, so no sum depends on the order of the atomics: results are bitwise
+//   reproducible and the pairwise forces cancel exactly (total momentum).
 // k_finalize: fixed-point sums -> FP32 force (+ body force), final half-kick, sums cleared.
 #include "kernels.h"
 #include "pair.cuh"
 
 namespace mdpd {
 
-constexpr int kWin = 64;                 // list entries staged per lane per window
-constexpr double kFix = 4294967296.0;    // 2^32
+constexpr int kGather = 8;                       // neighbour positions in flight per lane
+constexpr float kFixF = 4294967296.0f;           // 2^32
 constexpr double kFixInv = 1.0 / 4294967296.0;
+constexpr float kFixMax = 1.0e9f;                // |F| bound of the fixed-point range (2^63 / 2^32)
 
 template <bool HALF>
-__global__ void __launch_bounds__(128, 8) k_density_staged(const BoxDesc *__restrict__ boxes,
-                                                            const Unit *__restrict__ units, int nunits)
+__global__ void __launch_bounds__(128, 8) k_density_rows(const BoxDesc *__restrict__ boxes,
+                                                      const Unit *__restrict__ units, int nunits)
 {
-    __shared__ int s_idx[4][kWin][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
-        const Unit U = units[u];
-        const BoxDesc &B = boxes[U.box];
-        const int i = U.begin + threadIdx.x;
-        const bool live = i < U.end;
-        const int c = B.st->cur;
-        const bool in_group = live && (B.mask[c][i] & B.rho_bit);
-        const int n = live ? B.count[i] : 0;
-        int nmax = n;
-        for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
-        const float4 pi = live ? B.pos[i] : make_float4(0, 0, 0, 0);
-        const float h = B.cut_rho, h2 = h * h, rcf2 = B.rc2_force;
-        const int ncol = B.n_col, ncol2 = B.n_col2, nlocal = B.nlocal;
-        // this lane's row base (locally transposed); i&~31 is the warp's block
-        const int *row = B.table + ((U.begin + (w << 5)) & ~31) * ncol + lane;
-        int *row2 = B.table2 + (i & ~31) * ncol2 + (i & 31);
-        float acc = 0.f;
-        int n2 = 0;
-        for (int kw = 0; kw < nmax; kw += kWin) {
-            const int kend = min(kw + kWin, nmax);
-            // stage the window: for a fixed k the 32 lanes read 128 contiguous bytes
+    const int u = blockIdx.x;
+    if (u >= nunits) return;
+    const int lane = threadIdx.x & 31;
+    const Unit U = units[u];
+    const BoxDesc &B = boxes[U.box];
+    const int i = U.begin + threadIdx.x;
+    const bool live = i < U.end;
+    const int c = B.st->cur;
+    const bool in_group = live && (B.mask[c][i] & B.rho_bit);
+    const int n = live ? B.count[i] : 0;
+    int nmax = n;
+    for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+    const float4 pi = live ? B.pos[i] : make_float4(0, 0, 0, 0);
+    const float h = B.cut_rho, h2 = h * h, rcf2 = B.rc2_force;
+    const int ncol = B.n_col, nlocal = B.nlocal;
+    const int *row = B.table + (i & ~31) * ncol + (i & 31);  // entry k at (k & 31) * ncol + (k & ~31)
+    const int ncol2 = B.n_col2;
+    int *row2 = B.table2 + (size_t)i * ncol2;
+    float acc = 0.f;
+    int n2 = 0;
+    for (int k0 = 0; k0 < nmax; k0 += kGather) {
+        int j[kGather];
+        float4 pj[kGather];
 #pragma unroll
-            for (int k0 = 0; k0 < kWin; k0 += 8) {
-                int v[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const int k = kw + k0 + q;
-                    v[q] = k < kend ? __ldcs(row + (k & 31) * ncol + (k & ~31)) : 0;
-                }
-#pragma unroll
-                for (int q = 0; q < 8; ++q) s_idx[w][k0 + q][lane] = v[q];
-            }
-            __syncwarp();
-            const int myend = min(kend, n);
-            for (int k0 = kw; k0 < myend; k0 += 8) {
-                int j[8];
-                float4 pj[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) j[q] = k0 + q < myend ? s_idx[w][k0 + q - kw][lane] : -1;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) pj[q] = j[q] >= 0 ? __ldg(&B.pos[j[q]]) : make_float4(1e30f, 0, 0, 0);
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const float dx = pi.x - pj[q].x, dy = pi.y - pj[q].y, dz = pi.z - pj[q].z;
-                    const float rsq = dist2(dx, dy, dz);
-                    if (rsq < h2 && rsq >= 1e-20f) {
-                        const float d = h - rsq * rsqrtf(rsq);  // FP32 rsqrt, as the reference
-                        acc = __fmaf_rn(d, d, acc);
-                    }
-                    if (HALF && rsq < rcf2) {
-                        const int jj = j[q];
-                        const int src = jj < nlocal ? jj : B.gsrc[jj - nlocal];
-                        if (src > i) {  // the pair is evaluated from its lower-index end
-                            if (n2 < ncol2) row2[(n2 & 31) * ncol2 + (n2 & ~31)] = jj;
-                            ++n2;
-                        }
-                    }
-                }
-            }
-            __syncwarp();
+        for (int q = 0; q < kGather; ++q) {
+            const int k = k0 + q;
+            j[q] = k < n ? __ldcs(row + (k & 31) * ncol + (k & ~31)) : -1;
         }
-        if (live) {
-            if (HALF) {
-                B.count2[i] = min(n2, ncol2);
-                if (n2 > ncol2) atomicOr(&B.st->status, kErrList2Overflow);
+#pragma unroll
+        for (int q = 0; q < kGather; ++q) pj[q] = j[q] >= 0 ? __ldg(&B.pos[j[q]]) : make_float4(1e30f, 0, 0, 0);
+#pragma unroll
+        for (int q = 0; q < kGather; ++q) {
+            const float dx = pi.x - pj[q].x, dy = pi.y - pj[q].y, dz = pi.z - pj[q].z;
+            const float rsq = dist2(dx, dy, dz);
+            if (rsq < h2 && rsq >= 1e-20f) {
+                const float d = h - rsq * rsqrtf(rsq);  // FP32 rsqrt, as the reference
+                acc = __fmaf_rn(d, d, acc);
             }
-            if (in_group) {
-                const float r = (float)(B.mass[ptype(pi)] * (double)B.rho_factor) * acc;
-                B.rho[i] = r;
-                if (i >= B.st->n_bulk) {
-                    const int g1 = min(B.gfirst[i + 1], B.ghost_cap);
-                    for (int g = B.gfirst[i]; g < g1; ++g) B.rho[B.nlocal + g] = r;
+            if (HALF) {
+                const int jj = j[q];
+                if (rsq < rcf2 && (jj < nlocal ? jj > i : (pflags(pj[q]) & kUpperImage) != 0)) {
+                    if (n2 < ncol2) row2[n2] = jj;
+                    ++n2;
                 }
             }
         }
     }
+    if (HALF && live) {
+        B.count2[i] = min(n2, ncol2);
+        if (n2 > ncol2) atomicOr(&B.st->status, kErrList2Overflow);
+    }
+    if (in_group) {
+        const float r = (float)(B.mass[ptype(pi)] * (double)B.rho_factor) * acc;
+        B.rho[i] = r;
+        if (i >= B.st->n_bulk) {
+            const int g1 = min(B.gfirst[i + 1], B.ghost_cap);
+            for (int g = B.gfirst[i]; g < g1; ++g) B.rho[B.nlocal + g] = r;
+        }
+    }
 }
 
-__device__ __forceinline__ long long to_fix(float v) { return __double2ll_rn((double)v * kFix); }
+__device__ __forceinline__ long long to_fix(float v) { return __float2ll_rn(v * kFixF); }
+
+// 64-bit fixed-point add into a shared (lo, hi) pair of 32-bit words with native 32-bit
+// atomics: the low word's wrap-arounds carry into the high word, so the pair ends as the exact
+// 64-bit sum (mod 2^64) whatever the order of the adds
+__device__ __forceinline__ void sadd64(unsigned *lo, unsigned *hi, long long q)
+{
+    const unsigned ql = (unsigned)q, qh = (unsigned)((unsigned long long)q >> 32);
+    const unsigned old = atomicAdd(lo, ql);
+    atomicAdd(hi, qh + (old + ql < old ? 1u : 0u));
+}
 
 template <bool EXACT, bool EV, bool UNI>
-__global__ void __launch_bounds__(128) k_force_half(const BoxDesc *__restrict__ boxes,
-                                                    const Unit *__restrict__ units, int nunits)
+__global__ void __launch_bounds__(128) k_force_pairs(const BoxDesc *__restrict__ boxes,
+                                                     const Unit *__restrict__ units, int nunits)
 {
     __shared__ PairCoeff s_coeff[kMaxTypes * kMaxTypes];
+    __shared__ float4 s_pi[128], s_vi[128];
+    __shared__ float s_rho[128];
+    __shared__ int s_pre[4][33];
+    __shared__ unsigned s_lo[3][128], s_hi[3][128];
     __shared__ double s_red[4][7];
-    int cur_box = -1;
-    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
-        const Unit U = units[u];
-        const BoxDesc &B = boxes[U.box];
-        if (U.box != cur_box) {
-            __syncthreads();
-            for (int q = threadIdx.x; q < B.ntype * B.ntype; q += blockDim.x) s_coeff[q] = B.coeff[q];
-            cur_box = U.box;
-            __syncthreads();
-        }
-        const int i = U.begin + threadIdx.x;
-        const bool live = i < U.end;
-        long long fx = 0, fy = 0, fz = 0;
-        EvAcc ev = {0, 0, 0, 0, 0, 0, 0};
-        if (live) {
-            const int ntype = B.ntype, nlocal = B.nlocal;
-            const float4 pi = B.pos[i];
-            const float4 vi = B.vel[i];
-            const uint32_t si = __float_as_uint(vi.w);
-            const int ti = ptype(pi);
-            const float rho_i = B.rho[i];
-            const float dtis = B.dt_inv_sqrt;
-            const int n2 = B.count2[i];
-            const int ncol2 = B.n_col2;
-            const int *row2 = B.table2 + (i & ~31) * ncol2 + (i & 31);
-            unsigned long long *fax = B.facc, *fay = B.facc + nlocal, *faz = B.facc + 2 * nlocal;
-            int jn = n2 > 0 ? __ldcs(row2) : 0;
-            for (int k = 0; k < n2; ++k) {
-                const int j = jn;
-                const int kn = k + 1;
-                jn = kn < n2 ? __ldcs(row2 + (kn & 31) * ncol2 + (kn & ~31)) : 0;
-                const float4 pj = __ldg(&B.pos[j]);
-                const PairCoeff &cf = s_coeff[UNI ? 0 : ti * ntype + ptype(pj)];
-                float px = 0.f, py = 0.f, pz = 0.f;
-                pair_term<0, EXACT, EV, false>(B, cf, j, pj, pi, vi, si, rho_i, false, 1.f, 1.f, dtis, px, py, pz, ev);
-                const long long qx = to_fix(px), qy = to_fix(py), qz = to_fix(pz);
-                fx += qx, fy += qy, fz += qz;
-                const int src = j < nlocal ? j : B.gsrc[j - nlocal];
+    const int u = blockIdx.x;
+    if (u >= nunits) return;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5, wb = t & ~31;
+    const Unit U = units[u];
+    const BoxDesc &B = boxes[U.box];
+    for (int q = t; q < (UNI ? 1 : B.ntype * B.ntype); q += blockDim.x) s_coeff[q] = B.coeff[q];
+    const int i = U.begin + t;
+    const bool live = i < U.end;
+    int pre = 0;
+    if (live) {
+        s_pi[t] = B.pos[i];
+        s_vi[t] = B.vel[i];
+        s_rho[t] = B.rho[i];
+        pre = B.count2[i];
+    }
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, pre, o);
+        if (lane >= o) pre += v;
+    }
+    s_pre[w][lane + 1] = pre;
+    if (lane == 0) s_pre[w][0] = 0;
+    for (int c = 0; c < 3; ++c) s_lo[c][t] = s_hi[c][t] = 0u;
+    __syncthreads();
+    const int *P = s_pre[w];
+    const int T = P[32];
+    const int m0 = (lane * T) >> 5, m1 = ((lane + 1) * T) >> 5;
+    const int i0 = U.begin + wb, nlocal = B.nlocal, ntype = B.ntype, ncol2 = B.n_col2;
+    const float dtis = B.dt_inv_sqrt;
+    unsigned long long *fax = B.facc, *fay = B.facc + nlocal, *faz = B.facc + 2 * nlocal;
+    EvAcc ev = {0, 0, 0, 0, 0, 0, 0};
+    bool bad = false;
+    if (m0 < m1) {
+        int r = 0;  // the row holding entry m0: the last r with P[r] <= m0
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1)
+            if (P[r + st] <= m0) r += st;
+        int rbeg = P[r], rend = P[r + 1];
+        float4 pi = s_pi[wb + r], vi = s_vi[wb + r];
+        float rho_i = s_rho[wb + r];
+        const int *row = B.table2 + (size_t)(i0 + r) * ncol2;
+        long long ax = 0, ay = 0, az = 0;
+        for (int m = m0; m < m1; ++m) {
+            if (m >= rend) {  // the share moves on to the next non-empty row
+                sadd64(&s_lo[0][wb + r], &s_hi[0][wb + r], ax);
+                sadd64(&s_lo[1][wb + r], &s_hi[1][wb + r], ay);
+                sadd64(&s_lo[2][wb + r], &s_hi[2][wb + r], az);
+                ax = ay = az = 0;
+                do {
+                    ++r;
+                    rbeg = rend;
+                    rend = P[r + 1];
+                } while (m >= rend);
+                pi = s_pi[wb + r], vi = s_vi[wb + r];
+                rho_i = s_rho[wb + r];
+                row = B.table2 + (size_t)(i0 + r) * ncol2;
+            }
+            const int j = __ldcs(row + (m - rbeg));
+            const float4 pj = __ldg(&B.pos[j]);
+            const PairCoeff &cf = s_coeff[UNI ? 0 : ptype(pi) * ntype + ptype(pj)];
+            float px = 0.f, py = 0.f, pz = 0.f;
+            pair_term<0, EXACT, EV, false>(B, cf, j, pj, pi, vi, __float_as_uint(vi.w), rho_i, false, 1.f, 1.f,
+                                           dtis, px, py, pz, ev);
+            bad |= !(fabsf(px) < kFixMax && fabsf(py) < kFixMax && fabsf(pz) < kFixMax);
+            const long long qx = to_fix(px), qy = to_fix(py), qz = to_fix(pz);
+            ax += qx, ay += qy, az += qz;
+            const int src = j < nlocal ? j : __ldg(&B.gsrc[j - nlocal]);
+            const int d = src - U.begin;
+            if ((unsigned)d < 128u) {  // one of this block's rows (src < nlocal, so d < U.end - U.begin)
+                sadd64(&s_lo[0][d], &s_hi[0][d], -qx);
+                sadd64(&s_lo[1][d], &s_hi[1][d], -qy);
+                sadd64(&s_lo[2][d], &s_hi[2][d], -qz);
+            } else {
                 atomicAdd(fax + src, (unsigned long long)(-qx));
                 atomicAdd(fay + src, (unsigned long long)(-qy));
                 atomicAdd(faz + src, (unsigned long long)(-qz));
             }
-            atomicAdd(fax + i, (unsigned long long)fx);
-            atomicAdd(fay + i, (unsigned long long)fy);
-            atomicAdd(faz + i, (unsigned long long)fz);
         }
-        if (EV) {
-            // every pair once, full weight (the reference halves each side's share)
-            double vals[7] = {ev.vxx, ev.vyy, ev.vzz, ev.vxy, ev.vxz, ev.vyz, ev.pe};
+        sadd64(&s_lo[0][wb + r], &s_hi[0][wb + r], ax);
+        sadd64(&s_lo[1][wb + r], &s_hi[1][wb + r], ay);
+        sadd64(&s_lo[2][wb + r], &s_hi[2][wb + r], az);
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&B.st->status, kErrNonFinite);
+    __syncthreads();
+    if (live) {
+        atomicAdd(fax + i, ((unsigned long long)s_hi[0][t] << 32) | s_lo[0][t]);
+        atomicAdd(fay + i, ((unsigned long long)s_hi[1][t] << 32) | s_lo[1][t]);
+        atomicAdd(faz + i, ((unsigned long long)s_hi[2][t] << 32) | s_lo[2][t]);
+    }
+    if (EV) {
+        // every pair once, full weight (the reference halves each side's share)
+        double vals[7] = {ev.vxx, ev.vyy, ev.vzz, ev.vxy, ev.vxz, ev.vyz, ev.pe};
 #pragma unroll
-            for (int q = 0; q < 7; ++q)
-                for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_down_sync(0xffffffffu, vals[q], o);
-            if ((threadIdx.x & 31) == 0)
-                for (int q = 0; q < 7; ++q) s_red[threadIdx.x >> 5][q] = vals[q];
-            __syncthreads();
-            if (threadIdx.x < 7) {
-                double a = 0.0;
-                for (int ww = 0; ww < 4; ++ww) a += s_red[ww][threadIdx.x];
-                B.partial[(size_t)(U.begin / kUnit) * kPartialStride + 1 + threadIdx.x] = a;
-            }
-            __syncthreads();
+        for (int q = 0; q < 7; ++q)
+            for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_down_sync(0xffffffffu, vals[q], o);
+        if (lane == 0)
+            for (int q = 0; q < 7; ++q) s_red[w][q] = vals[q];
+        __syncthreads();
+        if (t < 7) {
+            double a = 0.0;
+            for (int ww = 0; ww < 4; ++ww) a += s_red[ww][t];
+            B.partial[(size_t)(U.begin / kUnit) * kPartialStride + 1 + t] = a;
         }
     }
 }
@@ -180,11 +222,13 @@ __global__ void __launch_bounds__(128) k_force_half(const BoxDesc *__restrict__ 
 __global__ void __launch_bounds__(kUnit) k_finalize(const BoxDesc *__restrict__ boxes,
                                                     const Unit *__restrict__ units, int nunits, int kick)
 {
-    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+    const int u = blockIdx.x;  // one unit per block: every load of the pass in flight at once
+    if (u >= nunits) return;
+    {
         const Unit U = units[u];
         const BoxDesc &B = boxes[U.box];
         const int i = U.begin + threadIdx.x;
-        if (i >= U.end) continue;
+        if (i >= U.end) return;
         const int c = B.st->cur, n = B.nlocal;
         unsigned long long *fa = B.facc;
         float fx = (float)((double)(long long)fa[i] * kFixInv);
@@ -208,26 +252,25 @@ __global__ void __launch_bounds__(kUnit) k_finalize(const BoxDesc *__restrict__ 
     }
 }
 
-void launch_density_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c)
+void launch_density_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &)
 {
-    const int grid = u.local.n < c.sms * 8 ? (u.local.n > 0 ? u.local.n : 1) : c.sms * 8;
-    k_density_staged<true><<<grid, 128, 0, s>>>(boxes, u.local.d, u.local.n);
+    if (u.local.n > 0) k_density_rows<true><<<u.local.n, 128, 0, s>>>(boxes, u.local.d, u.local.n);
 }
 
 void launch_force_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev, int kick)
 {
-    const int grid = u.local.n < c.sms * 16 ? (u.local.n > 0 ? u.local.n : 1) : c.sms * 16;
+    const int g = u.local.n;
+    if (g <= 0) return;
     if (c.exact_rng) {
-        if (ev) k_force_half<true, true, false><<<grid, 128, 0, s>>>(boxes, u.local.d, u.local.n);
-        else if (c.uniform_types) k_force_half<true, false, true><<<grid, 128, 0, s>>>(boxes, u.local.d, u.local.n);
-        else k_force_half<true, false, false><<<grid, 128, 0, s>>>(boxes, u.local.d, u.local.n);
+        if (ev) k_force_pairs<true, true, false><<<g, 128, 0, s>>>(boxes, u.local.d, g);
+        else if (c.uniform_types) k_force_pairs<true, false, true><<<g, 128, 0, s>>>(boxes, u.local.d, g);
+        else k_force_pairs<true, false, false><<<g, 128, 0, s>>>(boxes, u.local.d, g);
     } else {
-        if (ev) k_force_half<false, true, false><<<grid, 128, 0, s>>>(boxes, u.local.d, u.local.n);
-        else if (c.uniform_types) k_force_half<false, false, true><<<grid, 128, 0, s>>>(boxes, u.local.d, u.local.n);
-        else k_force_half<false, false, false><<<grid, 128, 0, s>>>(boxes, u.local.d, u.local.n);
+        if (ev) k_force_pairs<false, true, false><<<g, 128, 0, s>>>(boxes, u.local.d, g);
+        else if (c.uniform_types) k_force_pairs<false, false, true><<<g, 128, 0, s>>>(boxes, u.local.d, g);
+        else k_force_pairs<false, false, false><<<g, 128, 0, s>>>(boxes, u.local.d, g);
     }
-    const int g2 = u.local.n < c.sms * 8 ? (u.local.n > 0 ? u.local.n : 1) : c.sms * 8;
-    k_finalize<<<g2, kUnit, 0, s>>>(boxes, u.local.d, u.local.n, kick);
+    k_finalize<<<g, kUnit, 0, s>>>(boxes, u.local.d, g, kick);
 }
 
 }  // namespace mdpd

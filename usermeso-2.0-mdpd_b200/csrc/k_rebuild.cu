@@ -389,9 +389,10 @@ __global__ void __launch_bounds__(kUnit) k_rb_ghosts(const BoxDesc *__restrict__
                     const double gz = x[2] + sz * B.prd[2];
                     const int gi = B.nlocal + g;
                     B.gsrc[g] = k;
-                    B.gimg[g] = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
+                    const int code = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
+                    B.gimg[g] = code;
                     B.pos[gi] = make_float4((float)(gx - B.cen[0]), (float)(gy - B.cen[1]),
-                                            (float)(gz - B.cen[2]), w);
+                                            (float)(gz - B.cen[2]), ghost_w(w, code));
                     B.vel[gi] = vk;
                     const double gc[3] = {gx, gy, gz};
                     int bid[3];

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kUnit) k_integrate(BoxDesc *__restrict__ boxes
                     B.pos[B.nlocal + g] =
                         make_float4((float)(x + (code % 3 - 1) * B.prd[0] - B.cen[0]),
                                     (float)(y + ((code / 3) % 3 - 1) * B.prd[1] - B.cen[1]),
-                                    (float)(z + (code / 9 - 1) * B.prd[2] - B.cen[2]), w);
+                                    (float)(z + (code / 9 - 1) * B.prd[2] - B.cen[2]), ghost_w(w, code));
                     B.vel[B.nlocal + g] = vv;
                 }
             }

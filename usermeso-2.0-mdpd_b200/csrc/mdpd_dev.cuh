@@ -314,7 +314,18 @@ __device__ __forceinline__ int bin_coord(double x, double lo, double inv)
 __device__ __forceinline__ int ptype(const float4 &p) { return __float_as_int(p.w) & 0xFF; }
 __device__ __forceinline__ int pflags(const float4 &p) { return __float_as_int(p.w) >> 8; }
 
-// packed .w word of a position: type-1 in bits 0-7, mobile bit 8, wall bit 9
+// pflags bit of a ghost image shifted in the positive direction (image code > 13, i.e. the
+// shift (sx, sy, sz) is lexicographically positive in (sz, sy, sx)); the mirror image of a pair
+// seen from its other end has the opposite shift
+constexpr int kUpperImage = 4;
+
+__device__ __forceinline__ float ghost_w(float w, int code)
+{
+    return code > 13 ? __int_as_float(__float_as_int(w) | (kUpperImage << 8)) : w;
+}
+
+// packed .w word of a position: type-1 in bits 0-7, mobile bit 8, wall bit 9 (bit 10 on ghosts:
+// kUpperImage)
 __device__ __forceinline__ float pack_w(const BoxDesc &B, int type, int mask)
 {
     int w = (type - 1) & 0xFF;
