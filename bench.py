@@ -118,9 +118,10 @@ def peaks():
 
 
 def traffic_per_launch():
-    """DRAM bytes per launch of the force/density passes from the committed ncu summary."""
+    """DRAM bytes per step of the density and force passes (ncu capture of a 1M box, scaled
+    by particle count to the 4M box) from the committed profile summary."""
     try:
-        with open(os.path.join(ROOT, "profiles", "pair_passes_4M_ncu.json")) as f:
+        with open(os.path.join(ROOT, "profiles", "pair_passes_ncu.json")) as f:
             return json.load(f)
     except (OSError, ValueError):
         return None
@@ -279,7 +280,9 @@ def main():
         b4.setup()
         b4.step(args.equil)
         b4.step(args.warmup)
+        torch.cuda.nvtx.range_push("pair_profile")  # ncu --nvtx-include pair_profile/: the launch list
         prof = b4.profile(max(10, args.steps // 2))
+        torch.cuda.nvtx.range_pop()
         ms4 = b4.time(max(10, args.steps // 2))
         b4.close()
         peak, how = peaks()

@@ -430,101 +430,113 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__rest
 
 // ---------------------------------------------------------------------------
 // R11: neighbour list, warp per bin.  The 27 stencil bins are concatenated into one
-// candidate stream (lane = candidate, 32 per round); each of up to 32 centres of the bin
-// is tested against the round, hits are inserted by ballot in candidate order, and the
-// centre's running count lives in the register of the lane that owns that centre.
+// candidate stream (lane = candidate, 32 per round).  Each of up to 32 centres of the bin is
+// tested against the round; the ballot of centre c goes to shared memory, so after the round
+// each centre's lane reads the mask of its hits.  The lanes then write their hits in
+// candidate order, one per iteration of a loop as long as the largest mask.  Work items are
+// 8 bins (one per warp) of a 256-bin unit, taken grid-stride so every SM stays full whatever
+// the number of rebuilding boxes.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_rb_list(const BoxDesc *__restrict__ boxes,
+__global__ void __launch_bounds__(256, 5) k_rb_list(const BoxDesc *__restrict__ boxes,
                                                  const Unit *__restrict__ units, int nunits,
                                                  int nbox, int *done)
 {
-    __shared__ float4 s_c[8][32];   // centre position, .w = centre index
-    __shared__ int s_base[8][32];   // centre row base in the transposed table
+    __shared__ float4 s_c[8][32];   // centre position (far away in unused slots)
+    __shared__ unsigned s_bal[8][32];  // hit mask of centre c over the round's candidates
     __shared__ int s_bs[8][32], s_cum[8][33];
     const int lane = threadIdx.x & 31, w = threadIdx.x / 32;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
-        const Unit U = units[u];
+    const int nitems = nunits * 32;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const Unit U = units[it >> 5];
         const BoxDesc &B = boxes[U.box];
         if (!rebuilding(B)) continue;
+        const int b = U.begin + ((it & 31) << 3) + w;
+        if (b >= U.end) continue;
+        const int s = B.bin_start[b], e = B.bin_start[b + 1];
+        if (e == s || B.bin_order[s] >= B.nlocal) continue;  // no locals in this bin
         const float rc2 = B.rc2_tail;
         const int ncol = B.n_col, nlocal = B.nlocal;
+        const int bx = b % B.mbin[0], by = (b / B.mbin[0]) % B.mbin[1], bz = b / (B.mbin[0] * B.mbin[1]);
+        // stencil bins: lane l < 27 takes offset (l%3-1, l/3%3-1, l/9-1)
+        int st = 0, sz = 0;
+        if (lane < 27) {
+            const int x = bx + lane % 3 - 1, y = by + (lane / 3) % 3 - 1, z = bz + lane / 9 - 1;
+            if (x >= 0 && x < B.mbin[0] && y >= 0 && y < B.mbin[1] && z >= 0 && z < B.mbin[2]) {
+                const int nb = x + B.mbin[0] * (y + z * B.mbin[1]);
+                st = B.bin_start[nb];
+                sz = B.bin_start[nb + 1] - st;
+            }
+        }
+        int cum = sz;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, cum, o);
+            if (lane >= o) cum += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, cum, 31);
+        s_bs[w][lane] = st;
+        s_cum[w][lane + 1] = cum;
+        if (lane == 0) s_cum[w][0] = 0;
         int local_max = 0;
-        for (int b = U.begin + w; b < U.end; b += 8) {
-            const int s = B.bin_start[b], e = B.bin_start[b + 1];
-            if (e == s || B.bin_order[s] >= nlocal) continue;  // no locals in this bin
-            const int bx = b % B.mbin[0], by = (b / B.mbin[0]) % B.mbin[1], bz = b / (B.mbin[0] * B.mbin[1]);
-            // stencil bins: lane l < 27 takes offset (l%3-1, l/3%3-1, l/9-1)
-            int st = 0, sz = 0;
-            if (lane < 27) {
-                const int x = bx + lane % 3 - 1, y = by + (lane / 3) % 3 - 1, z = bz + lane / 9 - 1;
-                if (x >= 0 && x < B.mbin[0] && y >= 0 && y < B.mbin[1] && z >= 0 && z < B.mbin[2]) {
-                    const int nb = x + B.mbin[0] * (y + z * B.mbin[1]);
-                    st = B.bin_start[nb];
-                    sz = B.bin_start[nb + 1] - st;
-                }
-            }
-            int cum = sz;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, cum, o);
-                if (lane >= o) cum += v;
-            }
-            const int total = __shfl_sync(0xffffffffu, cum, 31);
-            s_bs[w][lane] = st;
-            s_cum[w][lane + 1] = cum;
-            if (lane == 0) s_cum[w][0] = 0;
+        __syncwarp();
+        for (int cb = s; cb < e; cb += 32) {
+            // centre batch: members with index < nlocal (they come first in a bin)
+            const int pc = cb + lane;
+            const int ci = pc < e ? B.bin_order[pc] : nlocal;
+            const bool is_c = ci < nlocal;
+            const unsigned cm = __ballot_sync(0xffffffffu, is_c);
+            if (cm == 0) break;
+            const int nc = __popc(cm);
+            s_c[w][lane] = is_c ? B.bpos[pc] : make_float4(3e30f, 3e30f, 3e30f, 0.f);
+            // row of this lane's centre in the locally transposed table
+            int *row = B.table + (ci & ~31) * ncol + (ci & 31);
+            int my_n = 0;
+            // this lane's centre appears in the candidate stream at slot 13 (the own bin)
+            const int q_self = s_cum[w][13] + (pc - s_bs[w][13]);
+            const int ncu = (nc + 3) & ~3;
             __syncwarp();
-            for (int cb = s; cb < e; cb += 32) {
-                // centre batch: members with index < nlocal (they come first in a bin)
-                const int pc = cb + lane;
-                const int ci = pc < e ? B.bin_order[pc] : nlocal;
-                const bool is_c = ci < nlocal;
-                const unsigned cm = __ballot_sync(0xffffffffu, is_c);
-                if (cm == 0) break;
-                const int nc = __popc(cm);
-                if (is_c) {
-                    float4 p = B.bpos[pc];
-                    p.w = __int_as_float(ci);
-                    s_c[w][lane] = p;
-                    s_base[w][lane] = (ci & ~31) * ncol + (ci & 31);
+            for (int q0 = 0; q0 < total; q0 += 32) {
+                const int q = q0 + lane;
+                float4 pj = make_float4(1e30f, 1e30f, 1e30f, 0.f);
+                int j = -1;
+                if (q < total) {
+                    int lo = 0, hi = 27;  // largest slot with s_cum[slot] <= q
+                    while (hi - lo > 1) {
+                        const int mid = (lo + hi) >> 1;
+                        if (s_cum[w][mid] <= q) lo = mid;
+                        else hi = mid;
+                    }
+                    const int p = s_bs[w][lo] + (q - s_cum[w][lo]);
+                    pj = B.bpos[p];
+                    j = B.bin_order[p];
                 }
-                int my_n = 0;  // running count of the centre owned by this lane
+#pragma unroll 4
+                for (int c = 0; c < ncu; ++c) {
+                    const float4 cc = s_c[w][c];
+                    const float r2 = dist2(cc.x - pj.x, cc.y - pj.y, cc.z - pj.z);
+                    const unsigned bal = __ballot_sync(0xffffffffu, r2 <= rc2);
+                    if (lane == 0) s_bal[w][c] = bal;
+                }
                 __syncwarp();
-                for (int q0 = 0; q0 < total; q0 += 32) {
-                    const int q = q0 + lane;
-                    const bool valid = q < total;
-                    float4 pj = make_float4(1e30f, 1e30f, 1e30f, 0.f);
-                    int j = -1;
-                    if (valid) {
-                        int lo = 0, hi = 27;  // largest slot with s_cum[slot] <= q
-                        while (hi - lo > 1) {
-                            const int mid = (lo + hi) >> 1;
-                            if (s_cum[w][mid] <= q) lo = mid;
-                            else hi = mid;
-                        }
-                        const int p = s_bs[w][lo] + (q - s_cum[w][lo]);
-                        pj = B.bpos[p];
-                        j = B.bin_order[p];
+                unsigned mine = lane < nc ? s_bal[w][lane] : 0u;
+                if ((unsigned)(q_self - q0) < 32u) mine &= ~(1u << (q_self - q0));  // not itself
+                const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(mine));
+                for (int r = 0; r < rounds; ++r) {
+                    const int src = mine ? __ffs(mine) - 1 : 0;
+                    const int jq = __shfl_sync(0xffffffffu, j, src);
+                    if (mine) {
+                        if (my_n < ncol) row[(my_n & 31) * ncol + (my_n & ~31)] = jq;
+                        ++my_n;
+                        mine &= mine - 1u;
                     }
-                    for (int c = 0; c < nc; ++c) {
-                        const float4 cc = s_c[w][c];
-                        const float r2 = dist2(cc.x - pj.x, cc.y - pj.y, cc.z - pj.z);
-                        const bool hit = r2 <= rc2 && j != __float_as_int(cc.w) && valid;
-                        const unsigned bal = __ballot_sync(0xffffffffu, hit);
-                        if (bal) {
-                            const int kq = __shfl_sync(0xffffffffu, my_n, c) + __popc(bal & lt);
-                            if (hit && kq < ncol) B.table[s_base[w][c] + (kq & 31) * ncol + (kq & ~31)] = j;
-                            if (lane == c) my_n += __popc(bal);
-                        }
-                    }
-                }
-                if (is_c) {
-                    B.count[ci] = my_n < ncol ? my_n : ncol;
-                    if (my_n > ncol) atomicOr(&B.st->status, kErrListOverflow);
-                    local_max = max(local_max, my_n);
                 }
                 __syncwarp();
             }
+            if (is_c) {
+                B.count[ci] = my_n < ncol ? my_n : ncol;
+                if (my_n > ncol) atomicOr(&B.st->status, kErrListOverflow);
+                local_max = max(local_max, my_n);
+            }
+            __syncwarp();
         }
         for (int o = 16; o > 0; o >>= 1) local_max = max(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
         if (lane == 0 && local_max > 0) atomicMax(&B.st->max_count, local_max);
@@ -562,7 +574,7 @@ void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const S
     scan<kSelBin>(s, boxes, u.scan_bin, u.nbox, sms);
     k_rb_scatter_bins<<<g(u.all.n, 8), kUnit, 0, s>>>(boxes, u.all.d, u.all.n);
     k_rb_bucket<1><<<g(u.bins.n, 4), 256, 0, s>>>(boxes, u.bins.d, u.bins.n);
-    k_rb_list<<<g(u.bins.n, 4), 256, 0, s>>>(boxes, u.bins.d, u.bins.n, u.nbox, done + 1);
+    k_rb_list<<<g(u.bins.n * 32, 5), 256, 0, s>>>(boxes, u.bins.d, u.bins.n, u.nbox, done + 1);
 }
 
 }  // namespace mdpd
