@@ -2,8 +2,10 @@
 density plateau and the surface tension gamma = (Lx/2)(Pxx - (Pyy+Pzz)/2), with the FP32
 random-number transform (default) against the bit-exact FP64 transform (pair_modify rng exact).
 
-Tolerances: T within 1% of kT; gamma > 0 and the two RNG modes agree within 2% of gamma or 3
-combined standard errors (block averages), whichever is larger; liquid plateau density within 2%.
+Tolerances: T within 2% of kT in each mode (the mDPD integrator bias at dt = 0.01, as the bulk
+liquid test) and the two modes' mean T within 0.5% or 3 combined standard errors of each other;
+gamma > 0 and the two RNG modes agree within 2% of gamma or 3 combined standard errors (block
+averages), whichever is larger; liquid plateau density within 2%.
 """
 import numpy as np
 import pytest
@@ -60,7 +62,8 @@ def test_slab_surface_tension_and_temperature():
     gf, tf, pf = slab("fast", 1111)
     ge, te, pe = slab("exact", 1111)
     for t in (tf, te):
-        assert abs(t.mean() - 1.0) < 0.01, t.mean()
+        assert abs(t.mean() - 1.0) < 0.02, (tf.mean(), te.mean())
+    assert abs(tf.mean() - te.mean()) < max(0.005, 3 * np.hypot(block_se(tf), block_se(te))), (tf.mean(), te.mean())
     assert gf.mean() > 0 and ge.mean() > 0
     tol = max(0.02 * abs(ge.mean()), 3 * np.hypot(block_se(gf), block_se(ge)))
     assert abs(gf.mean() - ge.mean()) < tol, (gf.mean(), ge.mean(), tol)

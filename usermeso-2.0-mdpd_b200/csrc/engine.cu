@@ -85,7 +85,7 @@ size_t Box::estimate_bytes(const Spec &spec, int n)
     b += (size_t)(n + gc) * (16 + 16 + 4 + 4 + 4 + 16 + 4);                      // pos, vel, rho, bin_of, bin_order, bpos, gfirst
     b += (size_t)gc * 8;
     b += (size_t)nrow * g.n_col * 4;
-    if (spec.style == 0) b += (size_t)nrow * (g.n_col2 + 1) * 4 + (size_t)n * 24;
+    if (spec.style == 0) b += (size_t)nrow * (g.n_col2 + 1) * 4 + (size_t)n * 24 + (size_t)(n + gc) * 16;
     b += (size_t)nbin * (4 + 3 * 4) * 3;
     b += (size_t)((n + kUnit - 1) / kUnit) * kPartialStride * 8;
     return b + (1u << 20);
@@ -193,6 +193,10 @@ Box::Box(const Spec &s, const Particles &p, int sms) : spec(s)
     }
 
     const int na = n + B.ghost_cap;
+    // the pair-once compact table packs j (27 bits) and j's type (3 bits) into one word
+    if (s.style == 0 && (long long)na >= (1LL << 27))
+        throw std::runtime_error("ARG: box too large for one device box: " + std::to_string(na) +
+                                 " particles and ghost images (limit 134217727)");
     for (int c = 0; c < 2; ++c) {
         for (int d = 0; d < 3; ++d) {
             B.x[c][d] = alloc<double>(n);
@@ -217,6 +221,7 @@ Box::Box(const Spec &s, const Particles &p, int sms) : spec(s)
         B.count2 = alloc<int>(B.nrow);
         B.table2 = alloc<int>((size_t)B.nrow * B.n_col2);
         B.facc = alloc<unsigned long long>(3 * (size_t)n);
+        B.posrho = alloc<float4>(na);
     }
     B.bin_rank = alloc<int>(nbin);
     B.cls_count = alloc<int>(2 * (size_t)nbin + 1);

@@ -6,10 +6,13 @@
 //   119-165) and writes, into the particle's row of the compact table, the entries within the
 //   force cutoff that the row owns: a local j when j > i, a ghost j when j is an image shifted
 //   in the positive direction (kUpperImage in pos.w). The mirrored pair, seen from the other
-//   end, has the opposite shift, so every pair is owned by exactly one row.
+//   end, has the opposite shift, so every pair is owned by exactly one row. It also writes
+//   (x, y, z, rho) of the particle and its ghost images for the force pass's gathers.
 // k_force_pairs: the 32 compact rows of a warp are concatenated and split into 32 equal
 //   contiguous shares, one per lane (a prefix scan of the row lengths and one binary search),
-//   so every lane evaluates the same number of pairs whatever the row lengths. The mDPD pair
+//   so every lane evaluates the same number of pairs whatever the row lengths. Each entry
+//   carries j's type; j's (x, y, z, rho) and velocity/signature are two float4 gathers, loaded
+//   for the next pair while the current one is evaluated. The mDPD pair
 //   force (pair_mdpd_meso.cu:139-225) is summed for the row in 64-bit fixed point (2^-32
 //   units) in registers and flushed when the lane's share moves to the next row; -F goes to
 //   j's source particle in the same fixed point, through shared memory when the source is
@@ -22,13 +25,18 @@
 
 namespace mdpd {
 
-constexpr int kGather = 8;                       // neighbour positions in flight per lane
+// neighbour positions in flight per lane, and the density pass's blocks per SM (64 registers):
+// 6 and 7 measured fastest on B200 against 4, 8 and 12 in flight
+constexpr int kGather = 6;
+constexpr int kDensityBlocks = 7;
 constexpr float kFixF = 4294967296.0f;           // 2^32
 constexpr double kFixInv = 1.0 / 4294967296.0;
 constexpr float kFixMax = 1.0e9f;                // |F| bound of the fixed-point range (2^63 / 2^32)
+constexpr int kEntryTypeShift = 27;              // compact entry: j | (type of j - 1) << 27
+constexpr int kEntryIndex = (1 << kEntryTypeShift) - 1;
 
 template <bool HALF>
-__global__ void __launch_bounds__(128, 8) k_density_rows(const BoxDesc *__restrict__ boxes,
+__global__ void __launch_bounds__(128, kDensityBlocks) k_density_rows(const BoxDesc *__restrict__ boxes,
                                                       const Unit *__restrict__ units, int nunits)
 {
     const int u = blockIdx.x;
@@ -72,7 +80,7 @@ __global__ void __launch_bounds__(128, 8) k_density_rows(const BoxDesc *__restri
             if (HALF) {
                 const int jj = j[q];
                 if (rsq < rcf2 && (jj < nlocal ? jj > i : (pflags(pj[q]) & kUpperImage) != 0)) {
-                    if (n2 < ncol2) row2[n2] = jj;
+                    if (n2 < ncol2) row2[n2] = jj | (ptype(pj[q]) << kEntryTypeShift);
                     ++n2;
                 }
             }
@@ -85,9 +93,16 @@ __global__ void __launch_bounds__(128, 8) k_density_rows(const BoxDesc *__restri
     if (in_group) {
         const float r = (float)(B.mass[ptype(pi)] * (double)B.rho_factor) * acc;
         B.rho[i] = r;
+        if (HALF) B.posrho[i] = make_float4(pi.x, pi.y, pi.z, r);
         if (i >= B.st->n_bulk) {
             const int g1 = min(B.gfirst[i + 1], B.ghost_cap);
-            for (int g = B.gfirst[i]; g < g1; ++g) B.rho[B.nlocal + g] = r;
+            for (int g = B.gfirst[i]; g < g1; ++g) {
+                B.rho[nlocal + g] = r;
+                if (HALF) {
+                    const float4 pg = B.pos[nlocal + g];
+                    B.posrho[nlocal + g] = make_float4(pg.x, pg.y, pg.z, r);
+                }
+            }
         }
     }
 }
@@ -139,8 +154,8 @@ __global__ void __launch_bounds__(128) k_force_pairs(const BoxDesc *__restrict__
     __syncthreads();
     const int *P = s_pre[w];
     const int T = P[32];
-    const int m0 = (lane * T) >> 5, m1 = ((lane + 1) * T) >> 5;
     const int i0 = U.begin + wb, nlocal = B.nlocal, ntype = B.ntype, ncol2 = B.n_col2;
+    const int m0 = (lane * T) >> 5, m1 = ((lane + 1) * T) >> 5;
     const float dtis = B.dt_inv_sqrt;
     unsigned long long *fax = B.facc, *fay = B.facc + nlocal, *faz = B.facc + 2 * nlocal;
     EvAcc ev = {0, 0, 0, 0, 0, 0, 0};
@@ -153,8 +168,12 @@ __global__ void __launch_bounds__(128) k_force_pairs(const BoxDesc *__restrict__
         int rbeg = P[r], rend = P[r + 1];
         float4 pi = s_pi[wb + r], vi = s_vi[wb + r];
         float rho_i = s_rho[wb + r];
-        const int *row = B.table2 + (size_t)(i0 + r) * ncol2;
         long long ax = 0, ay = 0, az = 0;
+        // j's state for the next entry is loaded while the current pair is evaluated
+        const int en = __ldcs(B.table2 + (size_t)(i0 + r) * ncol2 + (m0 - rbeg));
+        int jn = en & kEntryIndex, tn = en >> kEntryTypeShift;
+        float4 pjn = __ldg(&B.posrho[jn]), vjn = __ldg(&B.vel[jn]);
+        int srcn = jn < nlocal ? jn : __ldg(&B.gsrc[jn - nlocal]);
         for (int m = m0; m < m1; ++m) {
             if (m >= rend) {  // the share moves on to the next non-empty row
                 sadd64(&s_lo[0][wb + r], &s_hi[0][wb + r], ax);
@@ -168,18 +187,33 @@ __global__ void __launch_bounds__(128) k_force_pairs(const BoxDesc *__restrict__
                 } while (m >= rend);
                 pi = s_pi[wb + r], vi = s_vi[wb + r];
                 rho_i = s_rho[wb + r];
-                row = B.table2 + (size_t)(i0 + r) * ncol2;
             }
-            const int j = __ldcs(row + (m - rbeg));
-            const float4 pj = __ldg(&B.pos[j]);
-            const PairCoeff &cf = s_coeff[UNI ? 0 : ptype(pi) * ntype + ptype(pj)];
+            const int src = srcn, tj = tn;
+            const float4 pj = pjn, vj = vjn;  // pj.w: rho of j
+            if (m + 1 < m1) {
+                int rr = r, rb = rbeg, re = rend;  // entry m + 1: row r or a later non-empty row
+                while (m + 1 >= re) {
+                    ++rr;
+                    rb = re;
+                    re = P[rr + 1];
+                }
+                const int e = __ldcs(B.table2 + (size_t)(i0 + rr) * ncol2 + (m + 1 - rb));
+                const int jj = e & kEntryIndex;
+                tn = e >> kEntryTypeShift;
+                pjn = __ldg(&B.posrho[jj]);
+                vjn = __ldg(&B.vel[jj]);
+                srcn = jj < nlocal ? jj : __ldg(&B.gsrc[jj - nlocal]);
+            }
+            const PairCoeff &cf = s_coeff[UNI ? 0 : ptype(pi) * ntype + tj];
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float rsq = dist2(dx, dy, dz);
             float px = 0.f, py = 0.f, pz = 0.f;
-            pair_term<0, EXACT, EV, false>(B, cf, j, pj, pi, vi, __float_as_uint(vi.w), rho_i, false, 1.f, 1.f,
-                                           dtis, px, py, pz, ev);
+            if (rsq < cf.cutsq && rsq >= 1e-20f)
+                pair_core<0, EXACT, EV, false>(cf, dx, dy, dz, rsq, vi, vj, __float_as_uint(vi.w), rho_i, pj.w,
+                                               false, 1.f, 1.f, dtis, px, py, pz, ev);
             bad |= !(fabsf(px) < kFixMax && fabsf(py) < kFixMax && fabsf(pz) < kFixMax);
             const long long qx = to_fix(px), qy = to_fix(py), qz = to_fix(pz);
             ax += qx, ay += qy, az += qz;
-            const int src = j < nlocal ? j : __ldg(&B.gsrc[j - nlocal]);
             const int d = src - U.begin;
             if ((unsigned)d < 128u) {  // one of this block's rows (src < nlocal, so d < U.end - U.begin)
                 sadd64(&s_lo[0][d], &s_hi[0][d], -qx);

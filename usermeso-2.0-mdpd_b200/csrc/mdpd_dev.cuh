@@ -88,6 +88,7 @@ struct BoxDesc {
     // ---- packed FP32 state, locals then ghosts ----
     float4 *pos, *vel;
     float *rho;           // locals then ghosts
+    float4 *posrho;       // (x, y, z, rho) of locals then ghosts, written by the pair-once density pass
     float *phi[2];        // wall volume fraction of locals (double-buffered with x)
     int *gsrc, *gimg, *gfirst;
     // ---- neighbour list (locally transposed: 32-row blocks) ----
@@ -262,8 +263,8 @@ __device__ __forceinline__ double gaussian_exact(uint32_t si, uint32_t sj)
     return fmax(-4.0, fmin(g, 4.0));
 }
 
-// FP32 transform of the same TEA words (same polynomial for the angle; log of the radius
-// word through log1pf near 2^32 so a tiny radius keeps its relative accuracy)
+// FP32 transform of the same TEA words (same polynomial for the angle; the log of the radius
+// word keeps its relative accuracy near 2^32, where the radius is tiny)
 __device__ __forceinline__ float gaussian_fast(uint32_t si, uint32_t sj)
 {
     uint32_t v0 = max(si, sj), v1 = min(si, sj);
@@ -279,11 +280,21 @@ __device__ __forceinline__ float gaussian_fast(uint32_t si, uint32_t sj)
     s = __fmaf_rn(s, x2, -1.57079632662144460E+0f);
     const float f = (v0 & 0x80000000u) ? s * x : -s * x;
     const uint32_t w = max(v1, 1u);
-    // log2(w * 2^-32): log1p of the exact distance to 2^32 in the upper half (small |L|, where
-    // relative accuracy matters); the hardware log2 below 2^31, where |L| >= 1
-    const float l = w >= 0x80000000u ? log1pf(-(float)(0u - w) * 2.3283064365386963e-10f) * 1.4426950408889634f
-                                     : __log2f((float)w) - 32.0f;
-    const float a = (float)(-2.0 * 6.9314718055994528623E-1) * l;  // > 0: w <= 2^32 - 1
+    // a = -2 ln(w 2^-32) without a branch. Upper half (w >= 2^31): ln(1 - y) with the exact
+    // distance y = (2^32 - w) 2^-32 in (0, 1/2], as 2 atanh(s) = 2 (s + s^3/3 + ... + s^13/13),
+    // s = -y / (2 - y) in [-1/3, 0) (truncation below 1e-8); lower half: the hardware log2.
+    const float y = (float)(0u - w) * 2.3283064365386963e-10f;
+    const float sr = __fdividef(-y, 2.0f - y), t2 = sr * sr;
+    float ps = 1.0f / 13.0f;
+    ps = __fmaf_rn(ps, t2, 1.0f / 11.0f);
+    ps = __fmaf_rn(ps, t2, 1.0f / 9.0f);
+    ps = __fmaf_rn(ps, t2, 1.0f / 7.0f);
+    ps = __fmaf_rn(ps, t2, 1.0f / 5.0f);
+    ps = __fmaf_rn(ps, t2, 1.0f / 3.0f);
+    ps = __fmaf_rn(ps, t2, 1.0f);
+    const float a_hi = -4.0f * sr * ps;
+    const float a_lo = (__log2f((float)w) - 32.0f) * (float)(-2.0 * 6.9314718055994528623E-1);
+    const float a = w >= 0x80000000u ? a_hi : a_lo;
     const float r = a * rsqrtf(a);
     return fmaxf(-4.0f, fminf(r * f, 4.0f));
 }

@@ -9,18 +9,15 @@ struct EvAcc {
     float vxx, vyy, vzz, vxy, vxz, vyz, pe;
 };
 
-// one pair's contribution to particle i (pair_mdpd_meso.cu:139-225, pair_dpd_meso.cu:126-187);
-// returns without a contribution when the pair is outside the type-pair cutoff
+// one pair's contribution to particle i from the pair geometry and both particles' state
+// (pair_mdpd_meso.cu:139-225, pair_dpd_meso.cu:126-187); the caller has checked
+// cf.cutsq > rsq >= 1e-20
 template <int STYLE, bool EXACT, bool EV, bool WALLC>
-__device__ __forceinline__ void pair_term(const BoxDesc &B, const PairCoeff &cf, int j, const float4 &pj,
-                                          const float4 &pi, const float4 &vi, uint32_t si, float rho_i,
-                                          bool i_mobile, float wall_ratio, float wall_sqrt, float dtis, float &fx,
-                                          float &fy, float &fz, EvAcc &ev)
+__device__ __forceinline__ void pair_core(const PairCoeff &cf, float dx, float dy, float dz, float rsq,
+                                          const float4 &vi, const float4 &vj, uint32_t si, float rho_i,
+                                          float rho_j, bool wall_scaled, float wall_ratio, float wall_sqrt,
+                                          float dtis, float &fx, float &fy, float &fz, EvAcc &ev)
 {
-    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-    const float rsq = dist2(dx, dy, dz);
-    if (!(rsq < cf.cutsq && rsq >= 1e-20f)) return;
-    const float4 vj = __ldg(&B.vel[j]);
     const float rinv = rsqrtf(rsq);
     const float r = rsq * rinv;
     if (r < 1e-10f) return;
@@ -36,8 +33,7 @@ __device__ __forceinline__ void pair_term(const BoxDesc &B, const PairCoeff &cf,
     float fpair;
     if (STYLE == 0) {
         const float wcr = fmaxf(1.f - r * cf.inv_cut_r, 0.f);
-        const float rho_j = __ldg(&B.rho[j]);
-        if (WALLC && i_mobile && (pflags(pj) & 2)) {
+        if (WALLC && wall_scaled) {
             sig *= wall_sqrt;
             gam *= wall_ratio;
         }
@@ -60,6 +56,24 @@ __device__ __forceinline__ void pair_term(const BoxDesc &B, const PairCoeff &cf,
         ev.vxz += dx * dz * fpair;
         ev.vyz += dy * dz * fpair;
     }
+}
+
+// one pair's contribution to particle i, loading j's velocity and density only when the pair
+// is inside the type-pair cutoff
+template <int STYLE, bool EXACT, bool EV, bool WALLC>
+__device__ __forceinline__ void pair_term(const BoxDesc &B, const PairCoeff &cf, int j, const float4 &pj,
+                                          const float4 &pi, const float4 &vi, uint32_t si, float rho_i,
+                                          bool i_mobile, float wall_ratio, float wall_sqrt, float dtis, float &fx,
+                                          float &fy, float &fz, EvAcc &ev)
+{
+    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    const float rsq = dist2(dx, dy, dz);
+    if (!(rsq < cf.cutsq && rsq >= 1e-20f)) return;
+    const float4 vj = __ldg(&B.vel[j]);
+    const float rho_j = STYLE == 0 ? __ldg(&B.rho[j]) : 0.f;
+    pair_core<STYLE, EXACT, EV, WALLC>(cf, dx, dy, dz, rsq, vi, vj, si, rho_i, rho_j,
+                                       WALLC && i_mobile && (pflags(pj) & 2), wall_ratio, wall_sqrt, dtis, fx, fy,
+                                       fz, ev);
 }
 
 }  // namespace mdpd
