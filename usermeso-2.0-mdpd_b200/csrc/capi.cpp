@@ -25,6 +25,9 @@ struct mdpd_batch_s {
     std::vector<std::unique_ptr<Box>> boxes;
     std::unique_ptr<Batch> batch;
     std::string err;
+    int device = 0;
+    double *scratch = nullptr;  // device staging of state downloads, grown on demand
+    size_t scratch_bytes = 0;
 };
 
 static thread_local std::string g_err;
@@ -370,17 +373,13 @@ void spec_from_box(const mdpd_box_spec &bs, Spec &s, Particles &p)
     s.pair[0][0] = q;
     const int n = bs.n;
     p = Particles();
+    if (bs.x) return;  // the caller's arrays are used in place
     p.x.resize(3 * (size_t)n);
     p.v.resize(3 * (size_t)n);
     p.tag.resize(n);
     p.type.assign(n, 1);
     p.mask.assign(n, 1);
     for (int i = 0; i < n; ++i) p.tag[i] = i + 1;
-    if (bs.x) {
-        std::copy(bs.x, bs.x + 3 * (size_t)n, p.x.begin());
-        if (bs.v) std::copy(bs.v, bs.v + 3 * (size_t)n, p.v.begin());
-        return;
-    }
     std::mt19937_64 rng(bs.init_seed);
     std::uniform_real_distribution<double> u(0.0, 1.0);
     std::normal_distribution<double> g(0.0, 1.0);
@@ -414,7 +413,8 @@ int mdpd_batch_create(mdpd_batch_t **out, const mdpd_box_spec *specs, int32_t nb
     *out = nullptr;
     std::unique_ptr<mdpd_batch_s> b(new mdpd_batch_s);
     const int rc = guard(g_err, [&] {
-        check_cuda(cudaSetDevice(opts ? opts->device : 0), "set device");
+        b->device = opts ? opts->device : 0;
+        check_cuda(cudaSetDevice(b->device), "set device");
         StepConfig cfg;
         cfg.sms = sm_count();
         cfg.style = specs[0].style;
@@ -425,7 +425,10 @@ int mdpd_batch_create(mdpd_batch_t **out, const mdpd_box_spec *specs, int32_t nb
             Spec s;
             Particles p;
             spec_from_box(specs[k], s, p);
-            b->boxes.emplace_back(new Box(s, p, cfg.sms));
+            if (specs[k].x)  // the caller's arrays go to the device directly
+                b->boxes.emplace_back(new Box(s, specs[k].n, specs[k].x, specs[k].v, nullptr, nullptr, nullptr, cfg.sms));
+            else
+                b->boxes.emplace_back(new Box(s, p, cfg.sms));
             raw.push_back(b->boxes.back().get());
         }
         b->batch.reset(new Batch(raw, cfg));
@@ -471,16 +474,16 @@ int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int
     return guard(b->err, [&] {
         Box &bx = *b->boxes[box];
         if (n != bx.n) throw ScriptError(MDPD_ERR_ARG, "size mismatch");
-        std::vector<double> xi(3 * (size_t)n), vi(3 * (size_t)n);
-        std::vector<int32_t> tag(n);
-        bx.download_state(xi.data(), vi.data(), nullptr, tag.data(), nullptr, nullptr);
-        for (int i = 0; i < n; ++i) {
-            const int r = tag[i] - 1;
-            for (int d = 0; d < 3; ++d) {
-                if (x) x[3 * r + d] = xi[3 * i + d];
-                if (v) v[3 * r + d] = vi[3 * i + d];
-            }
+        check_cuda(cudaSetDevice(b->device), "set device");  // the gather runs on the batch's device
+        const size_t need = sizeof(double) * 6 * (size_t)n;
+        if (b->scratch_bytes < need) {
+            cudaFree(b->scratch);
+            b->scratch = nullptr;
+            b->scratch_bytes = 0;
+            check_cuda(cudaMalloc(&b->scratch, need), "download scratch");
+            b->scratch_bytes = need;
         }
+        bx.download_by_tag(x, v, b->scratch);
     });
 }
 
@@ -562,6 +565,7 @@ void mdpd_batch_destroy(mdpd_batch_t *b)
     if (!b) return;
     b->batch.reset();
     b->boxes.clear();
+    cudaFree(b->scratch);
     delete b;
 }
 

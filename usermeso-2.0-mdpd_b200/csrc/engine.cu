@@ -93,23 +93,90 @@ size_t Box::estimate_bytes(const Spec &spec, int n)
 
 template <class T> T *Box::alloc(size_t count)
 {
-    void *p = nullptr;
-    const size_t bytes_ = std::max<size_t>(count, 1) * sizeof(T);
-    cudaError_t e = cudaMalloc(&p, bytes_);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        throw std::runtime_error("OOM: cudaMalloc of " + std::to_string(bytes_) + " bytes failed");
+    const size_t bytes_ = (std::max<size_t>(count, 1) * sizeof(T) + 255) & ~size_t(255);
+    if (!arena_) {
+        arena_need_ += bytes_;
+        return nullptr;
     }
-    check_cuda(cudaMemset(p, 0, bytes_), "memset");
-    allocs_.push_back(p);
-    bytes += bytes_;
-    return (T *)p;
+    T *p = reinterpret_cast<T *>(arena_ + arena_off_);
+    arena_off_ += bytes_;
+    return p;
+}
+
+void Box::layout(const Spec &s, int na)
+{
+    BoxDesc &B = desc;
+    // the host-initialised arrays first, contiguous, so one copy uploads them all
+    for (int d = 0; d < 3; ++d) B.x[0][d] = alloc<double>(n);
+    for (int d = 0; d < 3; ++d) B.v[0][d] = alloc<double>(n);
+    for (int d = 0; d < 3; ++d) B.xh[d] = alloc<double>(n);
+    B.tag[0] = alloc<int>(n);
+    B.type[0] = alloc<int>(n);
+    B.mask[0] = alloc<int>(n);
+    for (int d = 0; d < 3; ++d) {
+        B.x[1][d] = alloc<double>(n);
+        B.v[1][d] = alloc<double>(n);
+    }
+    B.tag[1] = alloc<int>(n);
+    B.type[1] = alloc<int>(n);
+    B.mask[1] = alloc<int>(n);
+    for (int c = 0; c < 2; ++c) {
+        B.f[c] = alloc<float4>(n);
+        B.phi[c] = alloc<float>(n);
+    }
+    B.pos = alloc<float4>(na);
+    B.vel = alloc<float4>(na);
+    B.rho = alloc<float>(na);
+    B.gsrc = alloc<int>(B.ghost_cap);
+    B.gimg = alloc<int>(B.ghost_cap);
+    B.gfirst = alloc<int>(n + 1);
+    B.count = alloc<int>(B.nrow);
+    B.table = alloc<int>((size_t)B.nrow * B.n_col);
+    if (s.style == 0) {
+        B.count2 = alloc<int>(B.nrow);
+        B.table2 = alloc<int>((size_t)B.nrow * B.n_col2);
+        B.facc = alloc<unsigned long long>(3 * (size_t)n);
+        B.posrho = alloc<float4>(na);
+    }
+    B.bin_rank = alloc<int>(nbin);
+    B.cls_count = alloc<int>(2 * (size_t)nbin + 1);
+    B.cls_start = alloc<int>(2 * (size_t)nbin + 1);
+    B.cls_cursor = alloc<int>(2 * (size_t)nbin + 1);
+    B.cls_of = alloc<int>(n);
+    B.sub_of = alloc<int>(n);
+    B.perm = alloc<int>(n);
+    B.bin_of = alloc<int>(na);
+    B.bin_count = alloc<int>(nbin + 1);
+    B.bin_start = alloc<int>(nbin + 1);
+    B.bin_cursor = alloc<int>(nbin + 1);
+    B.bin_order = alloc<int>(na);
+    B.bpos = alloc<float4>(na);
+    const int nchunk = std::max({2 * nbin, n + 1, nbin}) / kScanChunk + 2;
+    B.scan_part = alloc<int>(nchunk);
+    B.partial = alloc<double>((size_t)((n + kUnit - 1) / kUnit) * kPartialStride);
+    d_state = alloc<BoxState>(1);
+    B.st = d_state;
 }
 
 Box::Box(const Spec &s, const Particles &p, int sms) : spec(s)
 {
     (void)sms;
     n = (int)p.size();
+    init(s, p.x.data(), p.v.data(), p.tag.data(), p.type.data(), p.mask.data());
+}
+
+Box::Box(const Spec &s, int n_, const double *x, const double *v, const int32_t *tag, const int32_t *type,
+         const int32_t *mask, int sms)
+    : spec(s)
+{
+    (void)sms;
+    n = n_;
+    init(s, x, v, tag, type, mask);
+}
+
+void Box::init(const Spec &s, const double *x, const double *v, const int32_t *tag, const int32_t *type,
+               const int32_t *mask)
+{
     if (n <= 0) throw std::runtime_error("ARG: box has no particles");
     if (s.ntype < 1 || s.ntype > kMaxTypes) throw std::runtime_error("ARG: 1..8 atom types supported");
     for (int a = 0; a < s.ntype; ++a)
@@ -197,50 +264,19 @@ Box::Box(const Spec &s, const Particles &p, int sms) : spec(s)
     if (s.style == 0 && (long long)na >= (1LL << 27))
         throw std::runtime_error("ARG: box too large for one device box: " + std::to_string(na) +
                                  " particles and ghost images (limit 134217727)");
-    for (int c = 0; c < 2; ++c) {
-        for (int d = 0; d < 3; ++d) {
-            B.x[c][d] = alloc<double>(n);
-            B.v[c][d] = alloc<double>(n);
+    layout(s, na);  // size the arena
+    {
+        void *a = nullptr;
+        const cudaError_t e = cudaMalloc(&a, arena_need_);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw std::runtime_error("OOM: cudaMalloc of " + std::to_string(arena_need_) + " bytes failed");
         }
-        B.f[c] = alloc<float4>(n);
-        B.tag[c] = alloc<int>(n);
-        B.type[c] = alloc<int>(n);
-        B.mask[c] = alloc<int>(n);
-        B.phi[c] = alloc<float>(n);
+        arena_ = static_cast<char *>(a);
     }
-    for (int d = 0; d < 3; ++d) B.xh[d] = alloc<double>(n);
-    B.pos = alloc<float4>(na);
-    B.vel = alloc<float4>(na);
-    B.rho = alloc<float>(na);
-    B.gsrc = alloc<int>(B.ghost_cap);
-    B.gimg = alloc<int>(B.ghost_cap);
-    B.gfirst = alloc<int>(n + 1);
-    B.count = alloc<int>(B.nrow);
-    B.table = alloc<int>((size_t)B.nrow * B.n_col);
-    if (s.style == 0) {
-        B.count2 = alloc<int>(B.nrow);
-        B.table2 = alloc<int>((size_t)B.nrow * B.n_col2);
-        B.facc = alloc<unsigned long long>(3 * (size_t)n);
-        B.posrho = alloc<float4>(na);
-    }
-    B.bin_rank = alloc<int>(nbin);
-    B.cls_count = alloc<int>(2 * (size_t)nbin + 1);
-    B.cls_start = alloc<int>(2 * (size_t)nbin + 1);
-    B.cls_cursor = alloc<int>(2 * (size_t)nbin + 1);
-    B.cls_of = alloc<int>(n);
-    B.sub_of = alloc<int>(n);
-    B.perm = alloc<int>(n);
-    B.bin_of = alloc<int>(na);
-    B.bin_count = alloc<int>(nbin + 1);
-    B.bin_start = alloc<int>(nbin + 1);
-    B.bin_cursor = alloc<int>(nbin + 1);
-    B.bin_order = alloc<int>(na);
-    B.bpos = alloc<float4>(na);
-    const int nchunk = std::max({2 * nbin, n + 1, nbin}) / kScanChunk + 2;
-    B.scan_part = alloc<int>(nchunk);
-    B.partial = alloc<double>((size_t)((n + kUnit - 1) / kUnit) * kPartialStride);
-    d_state = alloc<BoxState>(1);
-    B.st = d_state;
+    check_cuda(cudaMemset(arena_, 0, arena_need_), "memset");
+    layout(s, na);  // hand out the pieces
+    bytes = arena_need_;
 
     // Morton rank of every bin: reorder buckets are visited in Morton order of their bin
     {
@@ -253,27 +289,48 @@ Box::Box(const Spec &s, const Particles &p, int sms) : spec(s)
         for (int r = 0; r < nbin; ++r) rank[codes[r].second] = r;
         check_cuda(cudaMemcpy(B.bin_rank, rank.data(), sizeof(int) * nbin, cudaMemcpyHostToDevice), "upload");
     }
-    // initial state into buffer 0, component-separated
+    // initial state into buffer 0: the caller's AoS x and v go to the list table's space (unused
+    // until the first build, which writes every entry it later reads), a kernel splits them
+    // into x, xh and v components and fills tags/types/masks that were not given
     {
-        std::vector<double> col(n);
-        for (int d = 0; d < 3; ++d) {
-            for (int i = 0; i < n; ++i) col[i] = p.x[3 * i + d];
-            check_cuda(cudaMemcpy(B.x[0][d], col.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "upload");
-            check_cuda(cudaMemcpy(B.xh[d], col.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "upload");
-            for (int i = 0; i < n; ++i) col[i] = p.v[3 * i + d];
-            check_cuda(cudaMemcpy(B.v[0][d], col.data(), sizeof(double) * n, cudaMemcpyHostToDevice), "upload");
+        if (!x) throw std::runtime_error("ARG: no positions");
+        const size_t need = 6 * sizeof(double) * (size_t)n;
+        if ((size_t)B.nrow * B.n_col * sizeof(int) < need) throw std::runtime_error("ARG: list table too small to stage");
+        double *sx = reinterpret_cast<double *>(B.table), *sv = sx + 3 * (size_t)n;
+        check_cuda(cudaMemcpy(sx, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice), "upload");
+        if (v) check_cuda(cudaMemcpy(sv, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice), "upload");
+        if (tag) check_cuda(cudaMemcpy(B.tag[0], tag, sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
+        if (type) check_cuda(cudaMemcpy(B.type[0], type, sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
+        if (mask) check_cuda(cudaMemcpy(B.mask[0], mask, sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
+        launch_load_state(0, sx, v ? sv : nullptr, n, B.x[0], B.xh, B.v[0], tag ? nullptr : B.tag[0],
+                          type ? nullptr : B.type[0], mask ? nullptr : B.mask[0]);
+        check_cuda(cudaGetLastError(), "upload");
+        check_cuda(cudaStreamSynchronize(0), "upload");
+        if (mask) {
+            for (int i = 0; i < n; ++i)
+                if (mask[i] & s.nve_bit) ++n_group;
+        } else {
+            n_group = (1 & s.nve_bit) ? n : 0;
         }
-        check_cuda(cudaMemcpy(B.tag[0], p.tag.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
-        check_cuda(cudaMemcpy(B.type[0], p.type.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
-        check_cuda(cudaMemcpy(B.mask[0], p.mask.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
-        for (int i = 0; i < n; ++i)
-            if (p.mask[i] & s.nve_bit) ++n_group;
     }
 }
 
-Box::~Box()
+Box::~Box() { cudaFree(arena_); }
+
+void Box::download_by_tag(double *x, double *v, double *scratch) const
 {
-    for (void *p : allocs_) cudaFree(p);
+    const BoxState st = state();
+    const int c = st.cur;
+    double *d = scratch;
+    if (!d) check_cuda(cudaMalloc(&d, sizeof(double) * 6 * (size_t)n), "download");
+    launch_gather_by_tag(0, desc.x[c][0], desc.x[c][1], desc.x[c][2], desc.v[c][0], desc.v[c][1], desc.v[c][2],
+                         desc.tag[c], n, d, d + 3 * (size_t)n);
+    check_cuda(cudaGetLastError(), "download");
+    if (x) check_cuda(cudaMemcpyAsync(x, d, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, 0), "download");
+    if (v) check_cuda(cudaMemcpyAsync(v, d + 3 * (size_t)n, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, 0),
+                      "download");
+    check_cuda(cudaStreamSynchronize(0), "download");
+    if (!scratch) cudaFree(d);
 }
 
 BoxState Box::state() const
@@ -349,6 +406,7 @@ Batch::Batch(std::vector<Box *> boxes, const StepConfig &c) : cfg(c), boxes_(std
     check_cuda(cudaMalloc(&d_done, sizeof(int) * 4), "done");
     check_cuda(cudaMemset(d_done, 0, sizeof(int) * 4), "done");
     check_cuda(cudaMalloc(&d_thermo, sizeof(double) * kPartialStride * nb), "thermo");
+    check_cuda(cudaMalloc(&d_states, sizeof(BoxState) * nb), "states");
     build_units();
     capture(0);
     capture(1);
@@ -364,6 +422,7 @@ Batch::~Batch()
     cudaFree(d_boxes);
     cudaFree(d_done);
     cudaFree(d_thermo);
+    cudaFree(d_states);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -545,10 +604,12 @@ void Batch::thermo(std::vector<Thermo> &out)
     check_cuda(cudaMemcpyAsync(h.data(), d_thermo, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream_),
                "thermo download");
     check_cuda(cudaStreamSynchronize(stream_), "thermo");
+    std::vector<BoxState> sts;
+    read_states(sts);
     out.resize(nb);
     for (int b = 0; b < nb; ++b) {
         const Box &bx = *boxes_[b];
-        const BoxState st = bx.state();
+        const BoxState &st = sts[b];
         Thermo &t = out[b];
         const double *q = &h[(size_t)b * kPartialStride];
         t.step = st.step;
@@ -573,11 +634,24 @@ void Batch::thermo(std::vector<Thermo> &out)
     }
 }
 
+void Batch::read_states(std::vector<BoxState> &out)
+{
+    const int nb = (int)boxes_.size();
+    out.resize(nb);
+    launch_gather_states(stream_, d_boxes, nb, d_states);
+    check_cuda(cudaGetLastError(), "states launch");
+    check_cuda(cudaMemcpyAsync(out.data(), d_states, sizeof(BoxState) * nb, cudaMemcpyDeviceToHost, stream_),
+               "states download");
+    check_cuda(cudaStreamSynchronize(stream_), "states");
+}
+
 int Batch::status(std::string &msg)
 {
     int all = 0;
+    std::vector<BoxState> sts;
+    read_states(sts);
     for (size_t b = 0; b < boxes_.size(); ++b) {
-        const BoxState st = boxes_[b]->state();
+        const BoxState &st = sts[b];
         if (st.status) {
             all |= st.status;
             msg += "box " + std::to_string(b) + ": status " + std::to_string(st.status) + "; ";

@@ -60,6 +60,10 @@ struct Thermo {
 class Box {
 public:
     Box(const Spec &spec, const Particles &p, int sms);
+    // from caller arrays (AoS x[3n], v[3n]; v null: at rest; tag/type/mask null: tags 1..n,
+    // type 1, mask 1), copied straight to the device without host staging
+    Box(const Spec &spec, int n, const double *x, const double *v, const int32_t *tag, const int32_t *type,
+        const int32_t *mask, int sms);
     ~Box();
     Box(const Box &) = delete;
     Box &operator=(const Box &) = delete;
@@ -79,9 +83,19 @@ public:
     void download_state(double *x, double *v, double *f, int32_t *tag, int32_t *type,
                         int32_t *mask) const;           // current internal order
     void upload_xv(const double *x, const double *v);  // by tag, host order of tags 1..n
+    // positions and velocities in tag order (tags 1..n), gathered on the device and copied
+    // straight into x[3n] and v[3n] (either may be null)
+    // scratch: device memory of at least 48 n bytes (null: allocated and freed by the call)
+    void download_by_tag(double *x, double *v, double *scratch = nullptr) const;
 
 private:
-    std::vector<void *> allocs_;
+    // every device array of the box lives in one allocation: layout() runs twice, first to
+    // size the arena (alloc returns null), then to hand out 256-byte aligned pieces of it
+    char *arena_ = nullptr;
+    size_t arena_need_ = 0, arena_off_ = 0;
+    void layout(const Spec &s, int na);
+    void init(const Spec &s, const double *x, const double *v, const int32_t *tag, const int32_t *type,
+              const int32_t *mask);
     template <class T> T *alloc(size_t count);
 };
 
@@ -106,6 +120,7 @@ public:
     long long rebuild_steps();             // steps whose rebuild body ran (device counter)
     void thermo(std::vector<Thermo> &out); // reduce + download (synchronous)
     int status(std::string &msg);          // OR of box status words
+    void read_states(std::vector<BoxState> &out);  // every box's device scalars, one copy
     cudaStream_t stream() const { return stream_; }
     const std::vector<Box *> &boxes() const { return boxes_; }
     StepConfig cfg;
@@ -117,6 +132,7 @@ private:
     cudaStream_t stream_ = nullptr;
     int *d_done = nullptr;
     double *d_thermo = nullptr;
+    BoxState *d_states = nullptr;  // gathered copies of the boxes' scalars
     std::vector<Unit *> unit_allocs_;
     cudaGraphExec_t graph_[2] = {nullptr, nullptr};  // [ev]
     cudaGraph_t graph_src_[2] = {nullptr, nullptr};

@@ -520,6 +520,58 @@ __global__ void k_thermo_sum(const BoxDesc *__restrict__ boxes, int nbox, double
     }
 }
 
+__global__ void k_load_state(const double *__restrict__ xa, const double *__restrict__ va, int n, double *x0,
+                             double *x1, double *x2, double *h0, double *h1, double *h2, double *v0, double *v1,
+                             double *v2, int *tag, int *type, int *mask)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double a = xa[3 * i], b = xa[3 * i + 1], c = xa[3 * i + 2];
+    x0[i] = h0[i] = a, x1[i] = h1[i] = b, x2[i] = h2[i] = c;
+    v0[i] = va ? va[3 * i] : 0.0, v1[i] = va ? va[3 * i + 1] : 0.0, v2[i] = va ? va[3 * i + 2] : 0.0;
+    if (tag) tag[i] = i + 1;
+    if (type) type[i] = 1;
+    if (mask) mask[i] = 1;
+}
+
+void launch_load_state(cudaStream_t s, const double *xa, const double *va, int n, double *const x[3],
+                       double *const xh[3], double *const v[3], int *tag, int *type, int *mask)
+{
+    if (n > 0)
+        k_load_state<<<(n + 255) / 256, 256, 0, s>>>(xa, va, n, x[0], x[1], x[2], xh[0], xh[1], xh[2], v[0], v[1],
+                                                      v[2], tag, type, mask);
+}
+
+__global__ void k_gather_states(const BoxDesc *__restrict__ boxes, int nbox, BoxState *__restrict__ out)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nbox) out[b] = *boxes[b].st;
+}
+
+void launch_gather_states(cudaStream_t s, const BoxDesc *boxes, int nbox, BoxState *out)
+{
+    if (nbox > 0) k_gather_states<<<(nbox + 127) / 128, 128, 0, s>>>(boxes, nbox, out);
+}
+
+__global__ void k_gather_by_tag(const double *__restrict__ x0, const double *__restrict__ x1,
+                                const double *__restrict__ x2, const double *__restrict__ v0,
+                                const double *__restrict__ v1, const double *__restrict__ v2,
+                                const int *__restrict__ tag, int n, double *__restrict__ xo, double *__restrict__ vo)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int r = tag[i] - 1;
+    if (r < 0 || r >= n) return;  // tags are 1..n by construction
+    xo[3 * r] = x0[i], xo[3 * r + 1] = x1[i], xo[3 * r + 2] = x2[i];
+    vo[3 * r] = v0[i], vo[3 * r + 1] = v1[i], vo[3 * r + 2] = v2[i];
+}
+
+void launch_gather_by_tag(cudaStream_t s, const double *x0, const double *x1, const double *x2, const double *v0,
+                          const double *v1, const double *v2, const int *tag, int n, double *xo, double *vo)
+{
+    if (n > 0) k_gather_by_tag<<<(n + 255) / 256, 256, 0, s>>>(x0, x1, x2, v0, v1, v2, tag, n, xo, vo);
+}
+
 void launch_thermo(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, double *out, int *)
 {
     const int grid = u.local.n < 148 * 8 ? (u.local.n > 0 ? u.local.n : 1) : 148 * 8;

@@ -54,6 +54,15 @@ void launch_force(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const Ste
                   int kick);
 void launch_density_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c);
 void launch_force_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev, int kick);
+// AoS x[3n] (and v[3n], or zero when null) -> components x[d], xh[d], v[d]; tags 1..n, type 1
+// and mask 1 into the arrays given (null: left as uploaded)
+void launch_load_state(cudaStream_t s, const double *xa, const double *va, int n, double *const x[3],
+                       double *const xh[3], double *const v[3], int *tag, int *type, int *mask);
+// copies of every box's BoxState into out[nbox]
+void launch_gather_states(cudaStream_t s, const BoxDesc *boxes, int nbox, BoxState *out);
+// x, v (component arrays, internal order) -> xo[3n], vo[3n] in tag order (tags 1..n)
+void launch_gather_by_tag(cudaStream_t s, const double *x0, const double *x1, const double *x2, const double *v0,
+                          const double *v1, const double *v2, const int *tag, int n, double *xo, double *vo);
 void launch_thermo(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, double *out, int *done);
 void launch_density_profile(cudaStream_t s, const BoxDesc *boxes, int box, const Unit *units,
                             int nunits, int dim, int groupbit, double lo, double inv, int nbin,

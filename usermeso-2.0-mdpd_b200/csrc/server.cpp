@@ -121,7 +121,10 @@ void mdpd_server_s::loop()
                     bs.v = j->v0.empty() ? nullptr : j->v0.data();
                 }
                 spec_from_box(bs, s, p);
-                j->box.reset(new Box(s, p, cfg.sms));
+                if (bs.x)
+                    j->box.reset(new Box(s, bs.n, bs.x, bs.v, nullptr, nullptr, nullptr, cfg.sms));
+                else
+                    j->box.reset(new Box(s, p, cfg.sms));
                 std::lock_guard<std::mutex> lk(mu);
                 j->state = 1;
                 j->start_s = now();
@@ -210,16 +213,9 @@ void mdpd_server_s::loop()
                 std::vector<double> xf, vf;
                 if (j->spec.keep_state && !fail) {
                     const int n = j->box->n;
-                    std::vector<double> xi(3 * (size_t)n), vi(3 * (size_t)n);
-                    std::vector<int32_t> tag(n);
-                    j->box->download_state(xi.data(), vi.data(), nullptr, tag.data(), nullptr, nullptr);
                     xf.resize(3 * (size_t)n);
                     vf.resize(3 * (size_t)n);
-                    for (int i = 0; i < n; ++i)
-                        for (int d = 0; d < 3; ++d) {
-                            xf[3 * (tag[i] - 1) + d] = xi[3 * i + d];
-                            vf[3 * (tag[i] - 1) + d] = vi[3 * i + d];
-                        }
+                    j->box->download_by_tag(xf.data(), vf.data());
                 }
                 std::lock_guard<std::mutex> lk(mu);
                 j->thermo = out;

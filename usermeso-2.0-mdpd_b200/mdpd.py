@@ -313,9 +313,16 @@ class Batch:
         self._check(lib().mdpd_batch_thermo(self.h, box, C.byref(t)))
         return t
 
-    def state(self, box):
+    def state(self, box, x=None, v=None):
+        """Positions and velocities of one box in tag order; x, v: optional preallocated
+        C-contiguous float64 (n, 3) arrays to fill (pinned ones make the copy a direct DMA)."""
         n = self.n[box]
-        x = np.zeros((n, 3)); v = np.zeros((n, 3))
+        if x is None:
+            x = np.empty((n, 3))  # every row is written
+        if v is None:
+            v = np.empty((n, 3))
+        assert x.shape == (n, 3) and v.shape == (n, 3) and x.dtype == np.float64 and v.dtype == np.float64
+        assert x.flags.c_contiguous and v.flags.c_contiguous
         self._check(lib().mdpd_batch_get_state(self.h, box, _ptr(x, C.c_double), _ptr(v, C.c_double), n))
         return x, v
 
