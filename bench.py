@@ -210,6 +210,7 @@ def main():
     b = mdpd.Batch(specs, device=local)
     b.setup()
     b.step(args.equil)  # relax the random start (untimed)
+    shape_density, shape_force = b.tune()  # project autotuner (39 untimed steps)
     b.step(args.warmup)
     r0 = b.rebuild_steps()
     barrier()
@@ -230,11 +231,13 @@ def main():
             "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 pair / f64 integrate", "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD, "boxes": 256, "particles_per_gpu": ntot,
-                       "start": f"uniform random positions, Maxwell velocities, {args.equil} untimed steps",
+                       "start": f"uniform random positions, Maxwell velocities, {args.equil} untimed steps, "
+                                "then the autotuner's 39 untimed steps",
                        "rebuild_steps_timed": r1 - r0,
                        "l2": "inputs larger than L2: state + lists of ~%d particles (%.1f GB)" % (
                            ntot, ntot * 1.1e-6),
-                       "parallelism": f"replicas x{world} (independent box sets)"},
+                       "parallelism": f"replicas x{world} (independent box sets)",
+                       "tuned": {"density_gathers_in_flight": shape_density, "force_lanes_per_warp_share": shape_force}},
             "clocks": clk.summary(), "gpu_launches": gpu_launches}
 
     if not args.no_extras and rank == 0:
@@ -259,20 +262,24 @@ def main():
               for c, x, v in zip(cfg, xin, vin)]
         be = mdpd.Batch(sp, device=local)
         be.setup()
+        t1 = time.perf_counter()
         temps = []
         for _ in range(args.steps):
             be.step(1)
             temps.append(be.thermo(0).temp)  # the step's result, read on the host
+        t2 = time.perf_counter()
         for k in range(len(cfg)):
             be.state(k, xout[k], vout[k])
         e2e_s = time.perf_counter() - t0
+        split = {"create_upload_setup_s": t1 - t0, "steps_s": t2 - t1, "download_s": e2e_s - (t2 - t0)}
         be.close()
         state_bytes = 48 * ntot
         line["e2e"] = {"value": ntot * args.steps / e2e_s, "unit": "particle-steps/s",
                        "h2d_bytes_per_step": int(state_bytes / args.steps),
                        "d2h_bytes_per_step": int(state_bytes / args.steps + ctypes.sizeof(mdpd.Thermo)),
                        "note": "wall clock of: create of all 256 boxes from pinned host x, v; setup; K steps, "
-                               "each followed by a thermo read; full state download into pinned host arrays"}
+                               "each followed by a thermo read; full state download into pinned host arrays",
+                       "split": split}
         del temps, xin, vin, xout, vout
 
         # ---- plain single-box path on the same boxes (one box per launch sequence) ----------

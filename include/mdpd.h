@@ -126,8 +126,12 @@ int mdpd_batch_setup(mdpd_batch_t *b);
 int mdpd_batch_step(mdpd_batch_t *b, int64_t nsteps);
 int mdpd_batch_thermo(mdpd_batch_t *b, int32_t box, mdpd_thermo_t *out);
 int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int64_t n);
-/* tune threads-per-particle of the pair passes by timing (project autotuner) */
-int mdpd_batch_tune(mdpd_batch_t *b, int32_t *tpp_density, int32_t *tpp_force);
+/* project autotuner: times the candidate shapes of the pair passes on this batch (13 real steps
+ * each, so the boxes advance) and keeps the fastest. Pair-once mDPD batches: *shape_density =
+ * neighbour gathers in flight per lane in the density pass (4, 6 or 8), *shape_force = 32 (a
+ * warp shares its 32 particles' pairs; fixed). Full-list batches (classic DPD, wall-coupled
+ * mDPD): threads per particle of the density and force passes (1, 2 or 4 each). */
+int mdpd_batch_tune(mdpd_batch_t *b, int32_t *shape_density, int32_t *shape_force);
 /* last per-step device time in milliseconds measured with CUDA events over nsteps */
 int mdpd_batch_time(mdpd_batch_t *b, int64_t nsteps, double *ms_per_step);
 /* nsteps un-captured steps with CUDA events around each kernel group (same kernels as the

@@ -86,3 +86,27 @@ def test_server_refuses_oversized_and_cancels():
     xa, va, _ = run_alone(sp[0], 40)
     assert np.array_equal(x, xa) and np.array_equal(v, va)
     srv.stop()
+
+
+def test_autotuner_picks_a_shape_and_keeps_the_physics():
+    # pair-once mDPD batch: the density pass's gathers in flight; full-list DPD batch: threads
+    # per particle. After tuning the batch keeps stepping with conserved momentum and no error.
+    b = mdpd.Batch(specs())
+    b.setup()
+    b.step(20)
+    g, f = b.tune()
+    assert g in (4, 6, 8) and f == 32
+    b.step(20)
+    for k in range(4):
+        t = b.thermo(k)
+        assert t.status == 0 and 0.5 < t.temp < 2.0
+        assert np.max(np.abs(t.momentum)) < 1e-6 * t.natoms
+    b.close()
+    d = mdpd.Batch([mdpd.box_spec(3000, 10.0, style=1, A=25.0, gamma=4.5, sigma=3.0, rho_est=0.0, seed=5,
+                                  init_seed=6)])
+    d.setup()
+    td, tf = d.tune()
+    assert td in (1, 2, 4) and tf in (1, 2, 4)
+    d.step(20)
+    assert d.thermo(0).status == 0
+    d.close()

@@ -509,36 +509,50 @@ int mdpd_batch_time(mdpd_batch_t *b, int64_t nsteps, double *ms)
     });
 }
 
-int mdpd_batch_tune(mdpd_batch_t *b, int32_t *tpp_density, int32_t *tpp_force)
+int mdpd_batch_tune(mdpd_batch_t *b, int32_t *shape_density, int32_t *shape_force)
 {
     if (!b) return MDPD_ERR_ARG;
     return guard(b->err, [&] {
         const StepConfig base = b->batch->cfg;
+        std::vector<StepConfig> cands;
+        if (base.half) {  // pair-once passes: the density pass's gathers in flight
+            for (int g : {4, 6, 8}) {
+                StepConfig c = base;
+                c.gather = g;
+                cands.push_back(c);
+            }
+        } else {  // full-list passes: threads per particle of each pass
+            for (int td : {1, 2, 4})
+                for (int tf : {1, 2, 4}) {
+                    StepConfig c = base;
+                    c.tpp_density = td;
+                    c.tpp_force = tf;
+                    cands.push_back(c);
+                }
+        }
         double best = 1e30;
         StepConfig pick = base;
-        for (int td : {1, 2, 4})
-            for (int tf : {1, 2, 4}) {
-                StepConfig c = base;
-                c.tpp_density = td;
-                c.tpp_force = tf;
-                b->batch->reconfigure(c);
-                b->batch->run(3, true);
-                cudaEvent_t e0, e1;
-                cudaEventCreate(&e0);
-                cudaEventCreate(&e1);
-                cudaEventRecord(e0, b->batch->stream());
-                b->batch->run(10, false);
-                cudaEventRecord(e1, b->batch->stream());
-                cudaEventSynchronize(e1);
-                float t = 0;
-                cudaEventElapsedTime(&t, e0, e1);
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                if (t < best) best = t, pick = c;
-            }
+        for (const StepConfig &c : cands) {
+            b->batch->reconfigure(c);
+            b->batch->run(3, true);
+            cudaEvent_t e0, e1;
+            check_cuda(cudaEventCreate(&e0), "event");
+            check_cuda(cudaEventCreate(&e1), "event");
+            cudaEventRecord(e0, b->batch->stream());
+            b->batch->run(10, false);
+            cudaEventRecord(e1, b->batch->stream());
+            cudaEventSynchronize(e1);
+            float t = 0;
+            cudaEventElapsedTime(&t, e0, e1);
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            if (t < best) best = t, pick = c;
+        }
         b->batch->reconfigure(pick);
-        if (tpp_density) *tpp_density = pick.tpp_density;
-        if (tpp_force) *tpp_force = pick.tpp_force;
+        if (shape_density) *shape_density = base.half ? pick.gather : pick.tpp_density;
+        if (shape_force) *shape_force = base.half ? 32 : pick.tpp_force;
+        std::string msg;
+        if (int st = b->batch->status(msg)) throw ScriptError(st & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, msg);
     });
 }
 

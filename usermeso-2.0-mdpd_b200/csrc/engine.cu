@@ -2,6 +2,8 @@
 // IF(rebuild){...} -> density -> force), setup and thermo.
 #include "engine.h"
 
+#include <mutex>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -89,6 +91,31 @@ size_t Box::estimate_bytes(const Spec &spec, int n)
     b += (size_t)nbin * (4 + 3 * 4) * 3;
     b += (size_t)((n + kUnit - 1) / kUnit) * kPartialStride * 8;
     return b + (1u << 20);
+}
+
+// Box arenas come from one stream-ordered pool per device that keeps freed memory mapped, so
+// boxes created after others were destroyed (a batch rebuilt by the server, a new batch after an
+// old one) do not pay for mapping fresh pages again. The pool is created on first use with the
+// device that is current.
+static cudaMemPool_t box_pool()
+{
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "device");
+    if (dev < 0 || dev >= 64) throw std::runtime_error("CUDA device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        check_cuda(cudaMemPoolCreate(&pools[dev], &props), "memory pool");
+        uint64_t keep = UINT64_MAX;
+        check_cuda(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep), "memory pool");
+    }
+    return pools[dev];
 }
 
 template <class T> T *Box::alloc(size_t count)
@@ -267,14 +294,14 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     layout(s, na);  // size the arena
     {
         void *a = nullptr;
-        const cudaError_t e = cudaMalloc(&a, arena_need_);
+        const cudaError_t e = cudaMallocFromPoolAsync(&a, arena_need_, box_pool(), 0);
         if (e != cudaSuccess) {
             cudaGetLastError();
-            throw std::runtime_error("OOM: cudaMalloc of " + std::to_string(arena_need_) + " bytes failed");
+            throw std::runtime_error("OOM: device allocation of " + std::to_string(arena_need_) + " bytes failed");
         }
         arena_ = static_cast<char *>(a);
     }
-    check_cuda(cudaMemset(arena_, 0, arena_need_), "memset");
+    check_cuda(cudaMemsetAsync(arena_, 0, arena_need_, 0), "memset");
     layout(s, na);  // hand out the pieces
     bytes = arena_need_;
 
@@ -315,7 +342,13 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     }
 }
 
-Box::~Box() { cudaFree(arena_); }
+Box::~Box()
+{
+    if (!arena_) return;
+    cudaDeviceSynchronize();  // no kernel of any stream may still use the arena
+    cudaFreeAsync(arena_, 0);
+    cudaStreamSynchronize(0);
+}
 
 void Box::download_by_tag(double *x, double *v, double *scratch) const
 {

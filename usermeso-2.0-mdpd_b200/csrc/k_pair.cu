@@ -25,18 +25,17 @@
 
 namespace mdpd {
 
-// neighbour positions in flight per lane, and the density pass's blocks per SM (64 registers):
-// 6 and 7 measured fastest on B200 against 4, 8 and 12 in flight
-constexpr int kGather = 6;
-constexpr int kDensityBlocks = 7;
+// the density pass keeps G neighbour positions in flight per lane (G = 4, 6 or 8, chosen per
+// batch by the autotuner; 6 measured fastest on a 4M box); blocks per SM at 64 registers
+template <int G> constexpr int density_blocks() { return G <= 4 ? 8 : 7; }
 constexpr float kFixF = 4294967296.0f;           // 2^32
 constexpr double kFixInv = 1.0 / 4294967296.0;
 constexpr float kFixMax = 1.0e9f;                // |F| bound of the fixed-point range (2^63 / 2^32)
 constexpr int kEntryTypeShift = 27;              // compact entry: j | (type of j - 1) << 27
 constexpr int kEntryIndex = (1 << kEntryTypeShift) - 1;
 
-template <bool HALF>
-__global__ void __launch_bounds__(128, kDensityBlocks) k_density_rows(const BoxDesc *__restrict__ boxes,
+template <bool HALF, int kGather>
+__global__ void __launch_bounds__(128, density_blocks<kGather>()) k_density_rows(const BoxDesc *__restrict__ boxes,
                                                       const Unit *__restrict__ units, int nunits)
 {
     const int u = blockIdx.x;
@@ -286,9 +285,15 @@ __global__ void __launch_bounds__(kUnit) k_finalize(const BoxDesc *__restrict__ 
     }
 }
 
-void launch_density_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &)
+void launch_density_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c)
 {
-    if (u.local.n > 0) k_density_rows<true><<<u.local.n, 128, 0, s>>>(boxes, u.local.d, u.local.n);
+    const int g = u.local.n;
+    if (g <= 0) return;
+    switch (c.gather) {
+    case 4: k_density_rows<true, 4><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
+    case 8: k_density_rows<true, 8><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
+    default: k_density_rows<true, 6><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
+    }
 }
 
 void launch_force_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev, int kick)

@@ -35,6 +35,7 @@ struct StepConfig {
     int uniform_types = 0; // every box has one atom type: constant coefficient index
     int half = 0;          // mdpd without wall coupling: each pair evaluated once (k_pair.cu)
     int half_enabled = 1;  // allow the half-list passes (set per batch from the boxes)
+    int gather = 6;        // pair-once density pass: neighbour positions in flight per lane (4, 6, 8)
     int sms = 148;
 };
 
