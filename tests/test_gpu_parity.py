@@ -271,3 +271,54 @@ def test_deterministic_replay():
         out.append((x, v))
         lam.close()
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_two_type_pair_once_force_and_density_match_oracle():
+    # the pair-once passes with two atom types (coefficients looked up per type pair, masses per
+    # type in the density): sigma = 0 forces and the density against the FP64 oracle
+    lam = mdpd.Lammps()
+    lam.commands("""
+units lj
+atom_style mdpd/atomic/meso 6.05
+neighbor 0.3 bin
+region box block 0 10 0 10 0 10 units box
+create_box 2 box
+create_atoms 1 random 4000 2468 box
+create_atoms 2 random 2000 1357 box
+mass 1 1.0
+mass 2 1.5
+velocity all create 1.0 97531 dist gaussian
+pair_style mdpd/meso 0.0 1.0 123456
+pair_coeff 1 1 -40 25 0.0 1.0 0.75
+pair_coeff 1 2 -30 20 0.0 1.0 0.70
+pair_coeff 2 2 -50 30 0.0 0.9 0.75
+fix BC all aboundary/rho/meso cut_rho 0.75
+fix NVE all nve/meso
+timestep 0.01
+run_style mvv/meso
+""")
+    lam.setup()
+    n = lam.natoms()
+    cnt, rows = gpu_rows(lam)
+    pos, vel = lam.field("pos4"), lam.field("vel4")
+    rho = lam.field("rho").astype(np.float64)
+    mass = np.zeros(8); mass[0], mass[1] = 1.0, 1.5
+    ref_rho = oracle.density(pos, cnt, rows, np.ones(n, np.int32), 1, 0.75, mass)
+    assert np.max(np.abs(rho[:n] - ref_rho) / ref_rho) < 5e-6
+    f = lam.field("force")[:, :3].astype(np.float64)
+    coeffs = {(0, 0): (1.0, 0.75, -40.0, 25.0, 0.0, 0.0), (0, 1): (1.0, 0.70, -30.0, 20.0, 0.0, 0.0),
+              (1, 0): (1.0, 0.70, -30.0, 20.0, 0.0, 0.0), (1, 1): (0.9, 0.75, -50.0, 30.0, 0.0, 0.0)}
+    ref = oracle.force_mdpd(pos, vel, rho, cnt, rows, coeffs, 0.01)
+    # |F| scale: the summed magnitudes of the conservative pair terms
+    typ = (pos[:, 3].view(np.int32) & 0xFF)
+    s = np.zeros(n)
+    for i in range(n):
+        js = rows[i, :cnt[i]]
+        d = pos[i, :3].astype(np.float64) - pos[js, :3].astype(np.float64)
+        r = np.sqrt((d * d).sum(1))
+        for jj, rr in zip(js, r):
+            c = coeffs[(int(typ[i]), int(typ[jj]))]
+            if 1e-10 < rr < c[0]:
+                s[i] += abs(c[2] * (1 - rr / c[0]) + c[3] * (rho[i] + rho[jj]) * max(1 - rr / c[1], 0))
+    err = np.abs(f - ref).max(1)
+    assert np.all(err <= 1e-5 * s + 1e-6), (err / (s + 1e-12)).max()
