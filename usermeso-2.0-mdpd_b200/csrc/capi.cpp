@@ -432,6 +432,11 @@ int mdpd_batch_create(mdpd_batch_t **out, const mdpd_box_spec *specs, int32_t nb
             raw.push_back(b->boxes.back().get());
         }
         b->batch.reset(new Batch(raw, cfg));
+        // staging for state downloads, sized once for the largest box
+        int nmax = 0;
+        for (Box *x : raw) nmax = std::max(nmax, x->n);
+        b->scratch_bytes = sizeof(double) * 6 * (size_t)nmax;
+        check_cuda(cudaMalloc(&b->scratch, b->scratch_bytes), "download scratch");
     });
     if (rc) return rc;
     *out = b.release();
