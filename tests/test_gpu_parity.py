@@ -322,3 +322,19 @@ run_style mvv/meso
                 s[i] += abs(c[2] * (1 - rr / c[0]) + c[3] * (rho[i] + rho[jj]) * max(1 - rr / c[1], 0))
     err = np.abs(f - ref).max(1)
     assert np.all(err <= 1e-5 * s + 1e-6), (err / (s + 1e-12)).max()
+
+
+@pytest.mark.parametrize("A", [float("inf"), -1e12])
+def test_nonfinite_or_out_of_range_force_reported(A):
+    # injected on the host through the coefficients: an infinite A gives non-finite forces, and
+    # A = -1e12 forces beyond the fixed-point sums' range (|F| < 1e9); both come back as
+    # MDPD_ERR_NAN from the call, the context stays usable
+    lam = mdpd_box(A=A)
+    with pytest.raises(mdpd.MdpdError) as e:
+        lam.setup()
+    assert e.value.code == mdpd.ERR_NAN
+    lam.close()
+    ok = mdpd_box()
+    ok.setup()
+    ok.step(2)
+    assert ok.thermo().status == 0
