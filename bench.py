@@ -223,7 +223,7 @@ def main():
     r1 = b.rebuild_steps()
     value, t_max = aggregate(ntot * args.steps, ms * args.steps / 1e3, world)
     gpu_launches = 3 * args.steps + 17 * (r1 - r0)
-    eq_states = [b.state(k) for k in range(len(cfg))] if (not args.no_extras and rank == 0) else None
+    eq_states = [b.state(k) for k in range(len(cfg))] if not args.no_extras else None
     b.close()
 
     line = {"metric": "mDPD particle-steps/s (batched 256-box workload)", "value": value,
@@ -240,9 +240,10 @@ def main():
                        "tuned": {"density_gathers_in_flight": shape_density, "force_lanes_per_warp_share": shape_force}},
             "clocks": clk.summary(), "gpu_launches": gpu_launches}
 
-    if not args.no_extras and rank == 0:
-        # ---- e2e through the C ABI: pinned host arrays in, every step's thermo read back,
-        # final state into pinned host arrays; creation, upload and setup inside the timing ----
+    if not args.no_extras:
+        # ---- e2e through the C ABI on every rank (its own box set): pinned host arrays in,
+        # every step's thermo read back, final state into pinned host arrays; creation, upload
+        # and setup inside the timing; particle-steps summed, wall time max over ranks ----
         import ctypes
         xs = [x for x, _ in eq_states]
         vs = [v for _, v in eq_states]
@@ -256,7 +257,7 @@ def main():
         vout = [pinned(v.shape) for v in vs]
         for a, b_ in zip(xin + vin, xs + vs):
             a[:] = b_
-        torch.cuda.synchronize()
+        barrier()
         t0 = time.perf_counter()
         sp = [mdpd.box_spec(c["n"], c["L"], A=c["A"], B=c["B"], cut_r=c["rd"], seed=c["seed"], x=x, v=v)
               for c, x, v in zip(cfg, xin, vin)]
@@ -274,14 +275,17 @@ def main():
         split = {"create_upload_setup_s": t1 - t0, "steps_s": t2 - t1, "download_s": e2e_s - (t2 - t0)}
         be.close()
         state_bytes = 48 * ntot
-        line["e2e"] = {"value": ntot * args.steps / e2e_s, "unit": "particle-steps/s",
-                       "h2d_bytes_per_step": int(state_bytes / args.steps),
-                       "d2h_bytes_per_step": int(state_bytes / args.steps + ctypes.sizeof(mdpd.Thermo)),
+        e2e_value, e2e_max_s = aggregate(ntot * args.steps, e2e_s, world)
+        all_state_bytes, _ = aggregate(state_bytes, 1.0, world)  # summed over ranks
+        line["e2e"] = {"value": e2e_value, "unit": "particle-steps/s",
+                       "h2d_bytes_per_step": int(all_state_bytes / args.steps),
+                       "d2h_bytes_per_step": int(all_state_bytes / args.steps + world * ctypes.sizeof(mdpd.Thermo)),
                        "note": "wall clock of: create of all 256 boxes from pinned host x, v; setup; K steps, "
                                "each followed by a thermo read; full state download into pinned host arrays",
                        "split": split}
         del temps, xin, vin, xout, vout
 
+    if not args.no_extras and rank == 0:
         # ---- plain single-box path on the same boxes (one box per launch sequence) ----------
         plain_ps, plain_s = 0.0, 0.0
         for c, x, v in zip(cfg, xs, vs):
