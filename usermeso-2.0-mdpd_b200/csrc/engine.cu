@@ -189,7 +189,12 @@ Box::Box(const Spec &s, const Particles &p, int sms) : spec(s)
 {
     (void)sms;
     n = (int)p.size();
-    init(s, p.x.data(), p.v.data(), p.tag.data(), p.type.data(), p.mask.data());
+    try {
+        init(s, p.x.data(), p.v.data(), p.tag.data(), p.type.data(), p.mask.data());
+    } catch (...) {
+        release();  // a constructor that throws runs no destructor
+        throw;
+    }
 }
 
 Box::Box(const Spec &s, int n_, const double *x, const double *v, const int32_t *tag, const int32_t *type,
@@ -198,7 +203,12 @@ Box::Box(const Spec &s, int n_, const double *x, const double *v, const int32_t 
 {
     (void)sms;
     n = n_;
-    init(s, x, v, tag, type, mask);
+    try {
+        init(s, x, v, tag, type, mask);
+    } catch (...) {
+        release();
+        throw;
+    }
 }
 
 void Box::init(const Spec &s, const double *x, const double *v, const int32_t *tag, const int32_t *type,
@@ -342,12 +352,15 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     }
 }
 
-Box::~Box()
+Box::~Box() { release(); }
+
+void Box::release() noexcept
 {
     if (!arena_) return;
     cudaDeviceSynchronize();  // no kernel of any stream may still use the arena
     cudaFreeAsync(arena_, 0);
     cudaStreamSynchronize(0);
+    arena_ = nullptr;
 }
 
 void Box::download_by_tag(double *x, double *v, double *scratch) const

@@ -94,6 +94,7 @@ private:
     char *arena_ = nullptr;
     size_t arena_need_ = 0, arena_off_ = 0;
     void layout(const Spec &s, int na);
+    void release() noexcept;  // returns the arena to the pool
     void init(const Spec &s, const double *x, const double *v, const int32_t *tag, const int32_t *type,
               const int32_t *mask);
     template <class T> T *alloc(size_t count);
