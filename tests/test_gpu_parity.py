@@ -338,3 +338,25 @@ def test_nonfinite_or_out_of_range_force_reported(A):
     ok.setup()
     ok.step(2)
     assert ok.thermo().status == 0
+
+
+def test_virial_and_pair_energy_match_oracle():
+    # thermo's virial tensor and pair energy (compute pressure/meso, pe/meso) after setup,
+    # against the oracle's per-atom sums over full rows (each pair twice at half weight; the
+    # pair-once pass adds each pair once at full weight); exact RNG, FP32 pair terms vs FP64
+    lam = mdpd_box(exact=True)
+    lam.setup()
+    t = lam.thermo()
+    cnt, rows = gpu_rows(lam)
+    pos, vel, rho = lam.field("pos4"), lam.field("vel4"), lam.field("rho").astype(np.float64)
+    sigma = np.sqrt(2 * 1.0 * 4.5)
+    coeffs = {(0, 0): (1.0, 0.75, -40.0, 25.0, 4.5, sigma)}
+    _, vir, ep = oracle.force_mdpd(pos, vel, rho, cnt, rows, coeffs, 0.01, ev=True)
+    vsum, vabs = vir.sum(0), np.abs(vir).sum(0)
+    assert np.all(np.abs(np.array(t.virial) - vsum) <= 1e-5 * vabs + 1e-6), (np.array(t.virial), vsum)
+    assert abs(t.pe - ep.sum()) <= 1e-5 * np.abs(ep).sum(), (t.pe, ep.sum())
+    # the scalar pressure from them (compute_pressure_meso.cu:121-150)
+    n = lam.natoms()
+    ke = t.ke
+    p_ref = (2 * ke + vsum[:3].sum()) / 3.0 / 1000.0
+    assert abs(t.press - p_ref) <= 1e-5 * (2 * ke + vabs[:3].sum()) / 3.0 / 1000.0 + 1e-9, (t.press, p_ref)
