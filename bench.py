@@ -285,7 +285,9 @@ def main():
                        "split": split}
         del temps, xin, vin, xout, vout
 
-    if not args.no_extras and rank == 0:
+    # per-GPU legs (plain path, pair-pass roofline, served jobs, CPU baseline): one GPU only, so a
+    # multi-GPU run holds its GPUs no longer than the timed and end-to-end legs need
+    if not args.no_extras and world == 1:
         # ---- plain single-box path on the same boxes (one box per launch sequence) ----------
         plain_ps, plain_s = 0.0, 0.0
         for c, x, v in zip(cfg, xs, vs):
