@@ -1,9 +1,10 @@
-"""mDPD liquid-vapour slab (the config-2 geometry, scaled down): temperature, the liquid
+"""mDPD liquid-vapour slab (the config-2 geometry scaled down, and at full size): temperature, the liquid
 density plateau and the surface tension gamma = (Lx/2)(Pxx - (Pyy+Pzz)/2), with the FP32
 random-number transform (default) against the bit-exact FP64 transform (pair_modify rng exact).
 
-Tolerances: T within 2% of kT in each mode (the mDPD integrator bias at dt = 0.01, as the bulk
-liquid test) and the two modes' mean T within 0.5% or 3 combined standard errors of each other;
+Tolerances: T within 2% of kT in each mode for the small slab (it carries a ~1% bias at
+dt = 0.01), within 1% at full size (108,900 particles, 18,000 sampled steps), and the two modes'
+mean T within 0.5% or 3 combined standard errors of each other;
 gamma > 0 and the two RNG modes agree within 2% of gamma or 3 combined standard errors (block
 averages), whichever is larger; liquid plateau density within 2%.
 """
@@ -71,3 +72,56 @@ def test_slab_surface_tension_and_temperature():
     top_f = np.sort(pf)[-8:].mean(); top_e = np.sort(pe)[-8:].mean()
     assert abs(top_f - top_e) / top_e < 0.02, (top_f, top_e)
     assert 5.0 < top_f < 8.0
+
+
+def slab_config2(rng_mode, seed, steps=20000, discard=2000, every=100):
+    """The config-2 slab at full size: box [-30,30]x[-15,15]x[-15,15], liquid |x| < 10 at
+    density 6.05 (108,900 particles), A=-40, B=25, r_c=1, r_d=0.75, gamma=4.5, kT=1, dt=0.01."""
+    lam = mdpd.Lammps()
+    lam.commands(f"""
+units lj
+atom_style mdpd/atomic/meso 6.05
+neighbor 0.3 bin
+neigh_modify every 1 delay 0 check yes
+region box block -30 30 -15 15 -15 15 units box
+create_box 1 box
+region liq block -10 10 -15 15 -15 15 units box
+create_atoms 1 random 108900 {seed} liq
+mass 1 1.0
+velocity all create 1.0 {seed + 1} dist gaussian
+pair_style mdpd/meso 1.0 1.0 {seed + 2}
+pair_coeff 1 1 -40 25 4.5 1.0 0.75
+pair_modify rng {rng_mode}
+fix BC all aboundary/rho/meso cut_rho 0.75
+fix NVE all nve/meso
+timestep 0.01
+run_style mvv/meso
+""")
+    lam.run(discard)
+    gam, tem, prof = [], [], []
+    for _ in range((steps - discard) // every):
+        lam.run(every)
+        t = lam.thermo()
+        gam.append(t.surface_tension)
+        tem.append(t.temp)
+    x, _, _, _ = lam.state()
+    h, _ = np.histogram(np.mod(x[:, 0] + 30.0, 60.0), bins=60, range=(0, 60))
+    prof = h / (30.0 * 30.0)
+    lam.close()
+    return np.array(gam), np.array(tem), prof
+
+
+def test_config2_slab_full_size():
+    # 20,000 steps, the first 2,000 discarded; block averages of 180 samples
+    gf, tf, pf = slab_config2("fast", 2024)
+    ge, te, pe = slab_config2("exact", 2024)
+    for t in (tf, te):  # the spec's bar at full size (the small slab above carries a ~1% bias)
+        assert abs(t.mean() - 1.0) < 0.01, (tf.mean(), te.mean())
+    assert abs(tf.mean() - te.mean()) < max(0.005, 3 * np.hypot(block_se(tf), block_se(te))), (tf.mean(), te.mean())
+    assert gf.mean() > 0 and ge.mean() > 0
+    tol = max(0.02 * abs(ge.mean()), 3 * np.hypot(block_se(gf), block_se(ge)))
+    assert abs(gf.mean() - ge.mean()) < tol, (gf.mean(), ge.mean(), tol)
+    # liquid plateau (the 14 central 1-wide bins of the 20-wide slab), both modes, within 2%
+    top_f = np.sort(pf)[-14:].mean(); top_e = np.sort(pe)[-14:].mean()
+    assert abs(top_f - top_e) / top_e < 0.02, (top_f, top_e)
+    assert 5.5 < top_f < 7.5
