@@ -360,3 +360,19 @@ def test_virial_and_pair_energy_match_oracle():
     ke = t.ke
     p_ref = (2 * ke + vsum[:3].sum()) / 3.0 / 1000.0
     assert abs(t.press - p_ref) <= 1e-5 * (2 * ke + vabs[:3].sum()) / 3.0 / 1000.0 + 1e-9, (t.press, p_ref)
+
+
+def test_body_force_adds_momentum_exactly():
+    # fix addforce/meso fx fy fz on the nve group: the pair forces cancel exactly in the
+    # fixed-point sums, so after t time units the mean velocity has grown by (fx, fy, fz) t / m
+    # up to the FP32 rounding of each particle's f + b (forces ~1e2 after equilibration: a
+    # random walk of ~1e-9 in the mean over 200 half-kicks)
+    lam = mdpd_box(extra="fix F all addforce/meso 0.02 -0.01 0.005")
+    lam.setup()
+    lam.step(300)  # past the random start's large forces, where FP32 f + b loses digits of b
+    _, v0, _, _ = lam.state()
+    lam.step(100)
+    _, v1, _, _ = lam.state()
+    dv = v1.mean(0) - v0.mean(0)
+    print("body force: mean dv - b t =", dv - np.array([0.02, -0.01, 0.005]))
+    assert np.allclose(dv, np.array([0.02, -0.01, 0.005]) * 100 * 0.01, rtol=0, atol=2e-8), dv

@@ -245,7 +245,18 @@ int mdpd_get_field(mdpd_t *h, const char *name, void *out, int64_t nbytes)
         if (f == "pos4") get(B.pos, 4);
         else if (f == "vel4") get(B.vel, 4);
         else if (f == "rho") get(B.rho, 4);
-        else if (f == "force") get(B.f[c], 4);
+        else if (f == "force") {  // after post_force, as the reference: pair force + body force
+            get(B.f[c], 4);
+            if (B.body_bit) {
+                std::vector<int> mask(cnt / 4);
+                check_cuda(cudaMemcpy(mask.data(), B.mask[c], sizeof(int) * mask.size(), cudaMemcpyDeviceToHost),
+                           "get field");
+                float *fo = static_cast<float *>(out);
+                for (size_t i = 0; i < mask.size(); ++i)
+                    if (mask[i] & B.body_bit)
+                        for (int d = 0; d < 3; ++d) fo[4 * i + d] = (float)((double)fo[4 * i + d] + B.body[d]);
+            }
+        }
         else if (f == "count") get(B.count, 4);
         else if (f == "tag") get(B.tag[c], 4);
         else if (f == "type") get(B.type[c], 4);

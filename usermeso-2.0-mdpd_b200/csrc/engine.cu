@@ -283,7 +283,7 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     B.cut_rho = (float)s.cut_rho;
     B.rho_factor = (float)(15.0 / (2.0 * M_PI * std::pow(s.cut_rho, 5.0)));
     B.body_bit = s.body_bit;
-    for (int d = 0; d < 3; ++d) B.body[d] = (float)s.body[d];
+    for (int d = 0; d < 3; ++d) B.body[d] = s.body[d];
     B.arb_bc = s.arb_bc;
     B.mobile_bit = s.mobile_bit;
     B.wall_bit = s.wall_bit;

@@ -19,7 +19,8 @@
 //   one of the block's 128 rows and global 64-bit atomics otherwise. Integer addition is
 //   associative, so no sum depends on the order of the atomics: results are bitwise
 //   reproducible and the pairwise forces cancel exactly (total momentum).
-// k_finalize: fixed-point sums -> FP32 force (+ body force), final half-kick, sums cleared.
+// k_finalize: fixed-point sums -> FP32 pair force, final half-kick (body force added in FP64),
+//   sums cleared.
 #include "kernels.h"
 #include "pair.cuh"
 
@@ -270,18 +271,14 @@ __global__ void __launch_bounds__(kUnit) k_finalize(const BoxDesc *__restrict__ 
         float fz = (float)((double)(long long)fa[2 * n + i] * kFixInv);
         fa[i] = 0ull, fa[n + i] = 0ull, fa[2 * n + i] = 0ull;
         const int m = B.mask[c][i];
-        if (m & B.body_bit) {
-            fx += B.body[0];
-            fy += B.body[1];
-            fz += B.body[2];
-        }
         if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&B.st->status, kErrNonFinite);
-        B.f[c][i] = make_float4(fx, fy, fz, 0.f);
+        B.f[c][i] = make_float4(fx, fy, fz, 0.f);  // the pair force; the body force is in the kicks
         if (kick && (m & B.nve_bit)) {
             const double dtfm = B.dtfm[B.type[c][i] - 1];
-            B.v[c][0][i] = __fma_rn(dtfm, (double)fx, B.v[c][0][i]);
-            B.v[c][1][i] = __fma_rn(dtfm, (double)fy, B.v[c][1][i]);
-            B.v[c][2][i] = __fma_rn(dtfm, (double)fz, B.v[c][2][i]);
+            const bool body = m & B.body_bit;
+            B.v[c][0][i] = __fma_rn(dtfm, (double)fx + (body ? B.body[0] : 0.0), B.v[c][0][i]);
+            B.v[c][1][i] = __fma_rn(dtfm, (double)fy + (body ? B.body[1] : 0.0), B.v[c][1][i]);
+            B.v[c][2][i] = __fma_rn(dtfm, (double)fz + (body ? B.body[2] : 0.0), B.v[c][2][i]);
         }
     }
 }

@@ -55,9 +55,12 @@ __global__ void __launch_bounds__(kUnit) k_integrate(BoxDesc *__restrict__ boxes
             if (m & B.nve_bit) {
                 const float4 f = B.f[c][i];
                 const double dtfm = B.dtfm[t - 1];
-                vx = __fma_rn(dtfm, (double)f.x, vx);
-                vy = __fma_rn(dtfm, (double)f.y, vy);
-                vz = __fma_rn(dtfm, (double)f.z, vz);
+                // the body force in FP64 (added to FP32 forces it would round the same way for
+                // every particle of a binade: a bias)
+                const bool body = m & B.body_bit;
+                vx = __fma_rn(dtfm, (double)f.x + (body ? B.body[0] : 0.0), vx);
+                vy = __fma_rn(dtfm, (double)f.y + (body ? B.body[1] : 0.0), vy);
+                vz = __fma_rn(dtfm, (double)f.z + (body ? B.body[2] : 0.0), vz);
                 x = __fma_rn(B.dtv, vx, x);
                 y = __fma_rn(B.dtv, vy, y);
                 z = __fma_rn(B.dtv, vz, z);
@@ -266,7 +269,7 @@ void launch_density(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const S
 // ---------------------------------------------------------------------------
 // force pass.  Per list entry: FP32 distance test against the type-pair cutoff; inside
 // it, the conservative + dissipative + random force with the pairwise gaussian of the
-// two signatures.  Epilogue (t==0): + body force, store f, final half-kick (FP64 v).
+// two signatures.  Epilogue (t==0): store f, final half-kick (FP64 v, body force in FP64).
 // ---------------------------------------------------------------------------
 constexpr int kQueue = 16;  // list entries tested per phase-1 round of the force pass
 
@@ -368,18 +371,14 @@ __global__ void __launch_bounds__(kUnit *TPP, 10 / TPP) k_force(const BoxDesc *_
         }
         if (live && t == 0) {
             const int m = B.mask[c][i];
-            if (m & B.body_bit) {
-                fx += B.body[0];
-                fy += B.body[1];
-                fz += B.body[2];
-            }
             if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&B.st->status, kErrNonFinite);
-            B.f[c][i] = make_float4(fx, fy, fz, 0.f);
+            B.f[c][i] = make_float4(fx, fy, fz, 0.f);  // the pair force; the body force is in the kicks
             if (kick && (m & B.nve_bit)) {
                 const double dtfm = B.dtfm[ptype(pi)];
-                B.v[c][0][i] = __fma_rn(dtfm, (double)fx, B.v[c][0][i]);
-                B.v[c][1][i] = __fma_rn(dtfm, (double)fy, B.v[c][1][i]);
-                B.v[c][2][i] = __fma_rn(dtfm, (double)fz, B.v[c][2][i]);
+                const bool body = m & B.body_bit;
+                B.v[c][0][i] = __fma_rn(dtfm, (double)fx + (body ? B.body[0] : 0.0), B.v[c][0][i]);
+                B.v[c][1][i] = __fma_rn(dtfm, (double)fy + (body ? B.body[1] : 0.0), B.v[c][1][i]);
+                B.v[c][2][i] = __fma_rn(dtfm, (double)fz + (body ? B.body[2] : 0.0), B.v[c][2][i]);
             }
         }
         if (EV) {

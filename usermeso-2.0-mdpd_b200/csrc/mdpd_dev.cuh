@@ -75,7 +75,7 @@ struct BoxDesc {
     int rho_bit;
     float cut_rho, rho_factor;   // 15/(2 pi cut_rho^5)
     int body_bit;
-    float body[3];
+    double body[3];       // fix addforce/meso: added in FP64 in both half-kicks (f holds the pair force)
     int arb_bc, mobile_bit, wall_bit;   // wall coupling (pair_style mdpd/meso ... fluid wall)
     int wall_fix;                        // aboundary bounce-back active
     float cut_phi, phi_factor, dw_factor, phi_c;

@@ -722,9 +722,10 @@ void Script::command(const std::string &raw)
             }
             rho_fix_ = id;
         } else if (style == "addforce/meso") {
-            if (narg != 6) parse_error("Illegal fix addforce/meso command");
+            // fix ID group addforce/meso fx fy fz; extra words are ignored (fix_addforce_meso.cu:37-48)
+            if (narg < 6) parse_error("Illegal fix addforce/meso command");
             spec_.body_bit = gb;
-            for (int d = 0; d < 3; ++d) spec_.body[d] = num(a[5 + d]);
+            for (int d = 0; d < 3; ++d) spec_.body[d] = num(a[4 + d]);
         } else if (style == "density/meso") {
             // MesoFixDensityProf ctor (fix_density_profile_meso.cpp:32-80)
             DensityFix d;
