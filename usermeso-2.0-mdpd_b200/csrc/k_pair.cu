@@ -266,19 +266,23 @@ __global__ void __launch_bounds__(kUnit) k_finalize(const BoxDesc *__restrict__ 
         if (i >= U.end) return;
         const int c = B.st->cur, n = B.nlocal;
         unsigned long long *fa = B.facc;
-        float fx = (float)((double)(long long)fa[i] * kFixInv);
-        float fy = (float)((double)(long long)fa[n + i] * kFixInv);
-        float fz = (float)((double)(long long)fa[2 * n + i] * kFixInv);
+        // every load of the particle is issued before the first store (the compiler may not move
+        // a load above a store to a possibly aliased array): one memory round trip, not four
+        const long long ax = (long long)fa[i], ay = (long long)fa[n + i], az = (long long)fa[2 * n + i];
+        const int m = B.mask[c][i], t = B.type[c][i];
+        const double vx = B.v[c][0][i], vy = B.v[c][1][i], vz = B.v[c][2][i];
+        const double dtfm = B.dtfm[t - 1];
+        const float fx = (float)((double)ax * kFixInv);
+        const float fy = (float)((double)ay * kFixInv);
+        const float fz = (float)((double)az * kFixInv);
         fa[i] = 0ull, fa[n + i] = 0ull, fa[2 * n + i] = 0ull;
-        const int m = B.mask[c][i];
         if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) atomicOr(&B.st->status, kErrNonFinite);
         B.f[c][i] = make_float4(fx, fy, fz, 0.f);  // the pair force; the body force is in the kicks
         if (kick && (m & B.nve_bit)) {
-            const double dtfm = B.dtfm[B.type[c][i] - 1];
             const bool body = m & B.body_bit;
-            B.v[c][0][i] = __fma_rn(dtfm, (double)fx + (body ? B.body[0] : 0.0), B.v[c][0][i]);
-            B.v[c][1][i] = __fma_rn(dtfm, (double)fy + (body ? B.body[1] : 0.0), B.v[c][1][i]);
-            B.v[c][2][i] = __fma_rn(dtfm, (double)fz + (body ? B.body[2] : 0.0), B.v[c][2][i]);
+            B.v[c][0][i] = __fma_rn(dtfm, (double)fx + (body ? B.body[0] : 0.0), vx);
+            B.v[c][1][i] = __fma_rn(dtfm, (double)fy + (body ? B.body[1] : 0.0), vy);
+            B.v[c][2][i] = __fma_rn(dtfm, (double)fz + (body ? B.body[2] : 0.0), vz);
         }
     }
 }

@@ -35,8 +35,21 @@ __device__ __forceinline__ bool last_block(int *done)
 // FP32 pack of locals and their ghost images.  The last block decides the rebuild
 // per box (LAMMPS Neighbor::decide) and sets the graph's conditional.
 // ---------------------------------------------------------------------------
+// resident blocks per SM of the integrate pass (the wall variant holds the wall normal sums)
+constexpr int integrate_blocks(bool wall) { return wall ? 5 : 8; }
+
+// packed position and velocity of ghost g, image `code` of a local at (x, y, z)
+__device__ __forceinline__ void put_ghost(const BoxDesc &B, int g, int code, double x, double y, double z,
+                                          float w, float4 vv)
+{
+    B.pos[B.nlocal + g] = make_float4((float)(x + (code % 3 - 1) * B.prd[0] - B.cen[0]),
+                                      (float)(y + ((code / 3) % 3 - 1) * B.prd[1] - B.cen[1]),
+                                      (float)(z + (code / 9 - 1) * B.prd[2] - B.cen[2]), ghost_w(w, code));
+    B.vel[B.nlocal + g] = vv;
+}
+
 template <bool WALL, int STYLE>
-__global__ void __launch_bounds__(kUnit) k_integrate(BoxDesc *__restrict__ boxes,
+__global__ void __launch_bounds__(kUnit, integrate_blocks(WALL)) k_integrate(BoxDesc *__restrict__ boxes,
                                                      const Unit *__restrict__ units, int nunits,
                                                      int nbox, int *done,
                                                      cudaGraphConditionalHandle cond, int use_cond)
@@ -48,13 +61,26 @@ __global__ void __launch_bounds__(kUnit) k_integrate(BoxDesc *__restrict__ boxes
         const int i = U.begin + threadIdx.x;
         bool moved = false;
         if (i < U.end) {
-            const long long step = B.st->step + 1;
-            const int t = B.type[c][i], m = B.mask[c][i];
+            // every load of the particle is issued before the first store (the compiler may not
+            // move a load above a store to a possibly aliased array): one memory round trip
+            const BoxState &S = *B.st;
+            const long long step = S.step + 1;
+            const int n_bulk = S.n_bulk;
+            const bool sn_cached = S.sn_ok && S.sn_step == step && S.sn_seed == B.seed;
+            const uint32_t sn_c = S.sn;
+            const int t = B.type[c][i], m = B.mask[c][i], tag = B.tag[c][i];
             double x = B.x[c][0][i], y = B.x[c][1][i], z = B.x[c][2][i];
             double vx = B.v[c][0][i], vy = B.v[c][1][i], vz = B.v[c][2][i];
+            const float4 f = B.f[c][i];
+            const double hx = B.xh[0][i], hy = B.xh[1][i], hz = B.xh[2][i];
+            const bool edge = i >= n_bulk;
+            const int g0 = edge ? B.gfirst[i] : 0;
+            const int g1 = edge ? min(B.gfirst[i + 1], B.ghost_cap) : 0;  // an overflowed build is reported, never written past
+            int code8[8];  // image codes of the first ghosts (7 at most unless a side is < 2 cutoffs)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) code8[q] = g0 + q < g1 ? B.gimg[g0 + q] : 13;
+            const double dtfm = B.dtfm[t - 1];
             if (m & B.nve_bit) {
-                const float4 f = B.f[c][i];
-                const double dtfm = B.dtfm[t - 1];
                 // the body force in FP64 (added to FP32 forces it would round the same way for
                 // every particle of a binade: a bias)
                 const bool body = m & B.body_bit;
@@ -114,29 +140,23 @@ __global__ void __launch_bounds__(kUnit) k_integrate(BoxDesc *__restrict__ boxes
             }
             B.v[c][0][i] = vx, B.v[c][1][i] = vy, B.v[c][2][i] = vz;
             B.x[c][0][i] = x, B.x[c][1][i] = y, B.x[c][2][i] = z;
-            const double ddx = x - B.xh[0][i], ddy = y - B.xh[1][i], ddz = z - B.xh[2][i];
+            const double ddx = x - hx, ddy = y - hy, ddz = z - hz;
             moved = ddx * ddx + ddy * ddy + ddz * ddz > B.triggersq;
             // pack
-            const uint32_t sn = seed_now(B.seed, step);
+            const uint32_t sn = sn_cached ? sn_c : seed_now(B.seed, step);  // box-uniform branch
             const float w = pack_w(B, t, m);
             const float4 p = make_float4((float)(x - B.cen[0]), (float)(y - B.cen[1]),
                                          (float)(z - B.cen[2]), w);
             const float fvx = (float)vx, fvy = (float)vy, fvz = (float)vz;
-            const int tag = B.tag[c][i];
             const uint32_t sg = STYLE == 0 ? sig_mdpd(tag, sn) : sig_dpd(tag, fvx, fvy, fvz, sn);
             const float4 vv = make_float4(fvx, fvy, fvz, __uint_as_float(sg));
             B.pos[i] = p;
             B.vel[i] = vv;
-            if (i >= B.st->n_bulk) {
-                const int g1 = min(B.gfirst[i + 1], B.ghost_cap);  // an overflowed build is reported, never written past
-                for (int g = B.gfirst[i]; g < g1; ++g) {
-                    const int code = B.gimg[g];
-                    B.pos[B.nlocal + g] =
-                        make_float4((float)(x + (code % 3 - 1) * B.prd[0] - B.cen[0]),
-                                    (float)(y + ((code / 3) % 3 - 1) * B.prd[1] - B.cen[1]),
-                                    (float)(z + (code / 9 - 1) * B.prd[2] - B.cen[2]), ghost_w(w, code));
-                    B.vel[B.nlocal + g] = vv;
-                }
+            if (edge) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (g0 + q < g1) put_ghost(B, g0 + q, code8[q], x, y, z, w, vv);
+                for (int g = g0 + 8; g < g1; ++g) put_ghost(B, g, B.gimg[g], x, y, z, w, vv);
             }
         }
         if (__syncthreads_or(moved) && threadIdx.x == 0) atomicOr(&B.st->moved, 1);
@@ -153,6 +173,11 @@ __global__ void __launch_bounds__(kUnit) k_integrate(BoxDesc *__restrict__ boxes
             S->rebuild = rb;
             S->ago = rb ? 0 : ago;
             S->step += 1;
+            // the next step's seed, once per box instead of once per particle (64 TEA rounds)
+            S->sn = seed_now(B.seed, S->step + 1);
+            S->sn_step = S->step + 1;
+            S->sn_seed = B.seed;
+            S->sn_ok = 1;
             any |= rb;
         }
         any = __syncthreads_or(any);
@@ -167,7 +192,8 @@ __global__ void __launch_bounds__(kUnit) k_integrate(BoxDesc *__restrict__ boxes
 void launch_integrate(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c,
                       int *done, cudaGraphConditionalHandle cond, int use_cond)
 {
-    int grid = u.local.n < c.sms * 8 ? u.local.n : c.sms * 8;
+    const int full = c.sms * integrate_blocks(c.wall);  // one resident wave, grid-stride over units
+    int grid = u.local.n < full ? u.local.n : full;
     if (grid < 1) grid = 1;
     if (c.wall) {
         if (c.style == 0)
