@@ -427,6 +427,29 @@ float orc_dr2f(float dx, float dy, float dz)
     return fmaf(dz, dz, fmaf(dx, dx, dy * dy));
 }
 
+/* The list a pair-once box keeps (the engine's reduction of the full list above, not a
+ * reference algorithm): of row i, the entries owned by i -- a local j > i, or a ghost image
+ * shifted in the positive direction (gimg > 13) -- and those within rn2 (squared, the FP32
+ * distance of the list test).  Row order is kept.  Row-major tables of ncol columns. */
+void orc_reduce_rows(int nlocal, int ncol, const int32_t *count, const int32_t *table,
+                     const float *pos4, const int32_t *gimg, float rn2, int32_t *out_count,
+                     int32_t *out_table)
+{
+    for (int i = 0; i < nlocal; ++i) {
+        const int32_t *row = table + (size_t)i * ncol;
+        int32_t *out = out_table + (size_t)i * ncol;
+        int m = 0;
+        for (int k = 0; k < count[i]; ++k) {
+            const int j = row[k];
+            const int owned = j < nlocal ? j > i : gimg[j - nlocal] > 13;
+            const float r2 = orc_dr2f(pos4[4 * i] - pos4[4 * j], pos4[4 * i + 1] - pos4[4 * j + 1],
+                                      pos4[4 * i + 2] - pos4[4 * j + 2]);
+            if (owned || r2 <= rn2) out[m++] = j;
+        }
+        out_count[i] = m;
+    }
+}
+
 typedef struct { uint64_t key; int bin; } stencil_t;
 
 static int stencil_cmp(const void *a, const void *b)

@@ -94,6 +94,9 @@ void orc_bin_ids(const orc_box *b, int nlocal, int nall, const double *x, const 
 /* full neighbor list (gpu_build_neighbor_list + join, neigh_build_meso.cu:17-127,188-232):
  * row-major table[i*n_col + k]; core (dr2 <= rc2_core) entries in stencil order first, then
  * skin entries in reverse stencil order.  Returns 0, or the first overflowing local + 1. */
+void orc_reduce_rows(int nlocal, int ncol, const int32_t *count, const int32_t *table,
+                     const float *pos4, const int32_t *gimg, float rn2, int32_t *out_count,
+                     int32_t *out_table);
 int orc_build_list(const orc_box *b, int nlocal, int nall, const double *x, const double *y,
                    const double *z, const float *pos4, int32_t *count, int32_t *count_core,
                    int32_t *table);

@@ -177,6 +177,20 @@ def pairs_from_rows(count, table, tags_local, gsrc):
     return np.concatenate(ti) if ti else np.zeros(0, np.int32), np.concatenate(tj) if tj else np.zeros(0, np.int32)
 
 
+def reduce_rows(count, table, pos4, gimg, rn2):
+    """Rows of a pair-once box: entries owned by the row's particle or within rn2 (FP32)."""
+    n, ncol = table.shape
+    count = np.ascontiguousarray(count, np.int32)
+    table = np.ascontiguousarray(table, np.int32)
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    gimg = np.ascontiguousarray(gimg, np.int32) if len(gimg) else np.zeros(1, np.int32)
+    oc = np.zeros(n, np.int32)
+    ot = np.zeros((n, ncol), np.int32)
+    lib().orc_reduce_rows(n, ncol, P(count, C.c_int32), P(table, C.c_int32), P(pos4, C.c_float),
+                          P(gimg, C.c_int32), C.c_float(rn2), P(oc, C.c_int32), P(ot, C.c_int32))
+    return oc, ot
+
+
 def density(pos4, count, table, mask, groupbit, cut_rho, mass_type):
     n = len(count)
     ncol = table.shape[1]

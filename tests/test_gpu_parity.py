@@ -105,13 +105,24 @@ def test_ghost_images_and_packed_positions_bit_exact():
     assert np.array_equal(pos[n + order, :3].view(np.uint32), ref["pos4"][n:, :3].view(np.uint32))
 
 
+# density cutoff + skin + 1e-3 (squared, FP32): the reduced rows of a pair-once mDPD box keep
+# the pairs within it and the pairs their particle owns
+RN2_LIST = np.float32((0.75 + 0.3 + 1e-3) ** 2)
+
+
 @pytest.mark.parametrize("n,L", [(6000, 10.0), (20000, 15.0)])
 def test_pair_sets_bit_exact(n, L):
+    # the reference's full list (oracle), reduced by the rule of a pair-once box: the entries
+    # owned by the row's particle (a local above it, an upper ghost image) and those within
+    # RN2_LIST; the other pairs reach neither the density sum nor the force pass before the
+    # next build (the full list itself is checked bit-exact on the DPD box below)
     lam = mdpd_box(n=n, L=L)
     ref, _, _ = oracle_rebuild(lam, L=L)
     lam.setup()
     ti, tj = lam.pairs()
-    ri, rj = oracle.pairs_from_rows(ref["count"], ref["table"], ref["tags"], ref["gsrc"])
+    cnt, tab = oracle.reduce_rows(ref["count"], ref["table"], ref["pos4"], ref["gimg"], RN2_LIST)
+    assert 0.7 * ref["count"].sum() < cnt.sum() < 0.85 * ref["count"].sum()
+    ri, rj = oracle.pairs_from_rows(cnt, tab, ref["tags"], ref["gsrc"])
     a = np.sort(ti.astype(np.int64) * (1 << 32) + tj)
     b = np.sort(ri.astype(np.int64) * (1 << 32) + rj)
     assert len(a) == len(b)
@@ -155,13 +166,16 @@ def gpu_rows(lam):
 
 
 def test_density_matches_oracle():
+    # over the reference's full rows (oracle), so that a neighbour missing from the device's
+    # rows would show
     lam = mdpd_box()
+    ref_rb, _, _ = oracle_rebuild(lam)
     lam.setup()
     n = lam.natoms()
-    cnt, rows = gpu_rows(lam)
     pos = lam.field("pos4")
     rho = lam.field("rho")
-    ref = oracle.density(pos, cnt, rows, np.ones(n, np.int32), 1, 0.75, np.ones(8))
+    ref = oracle.density(ref_rb["pos4"], ref_rb["count"], ref_rb["table"], np.ones(n, np.int32), 1, 0.75,
+                         np.ones(8))
     assert np.max(np.abs(rho[:n] - ref) / ref) < 5e-6
 
 

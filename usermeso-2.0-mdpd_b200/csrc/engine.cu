@@ -239,6 +239,11 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     B.triggersq = 0.25 * s.skin * s.skin;
     B.rc2_tail = g.rc2_tail;
     B.rc2_force = g.rc2_force;
+    {
+        const double rn = s.cut_rho + s.skin + 1e-3;
+        B.rn2_list = (float)(rn * rn);
+        B.list_reduce = 0;
+    }
     B.n_col2 = g.n_col2;
     nbin = B.nbin = g.mbin[0] * g.mbin[1] * g.mbin[2];
     B.nlocal = n;
@@ -301,6 +306,11 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     if (s.style == 0 && (long long)na >= (1LL << 27))
         throw std::runtime_error("ARG: box too large for one device box: " + std::to_string(na) +
                                  " particles and ghost images (limit 134217727)");
+    // the list kernels address the table with 32-bit offsets
+    if ((long long)B.nrow * B.n_col > 0x7fffffffLL)
+        throw std::runtime_error("ARG: box too large for one device box: " + std::to_string(n) + " particles need " +
+                                 std::to_string((long long)B.nrow * B.n_col) +
+                                 " neighbour-table entries (limit 2147483647); split it into boxes");
     layout(s, na);  // size the arena
     {
         void *a = nullptr;
@@ -447,7 +457,11 @@ Batch::Batch(std::vector<Box *> boxes, const StepConfig &c) : cfg(c), boxes_(std
     const int nb = (int)boxes_.size();
     check_cuda(cudaMalloc(&d_boxes, sizeof(BoxDesc) * nb), "boxes");
     std::vector<BoxDesc> h(nb);
-    for (int b = 0; b < nb; ++b) h[b] = boxes_[b]->desc;
+    for (int b = 0; b < nb; ++b) {
+        h[b] = boxes_[b]->desc;
+        // the reduced list serves the pair-once passes only (the wall fix reads the full list)
+        h[b].list_reduce = cfg.half && !cfg.wall && !h[b].wall_fix && h[b].rn2_list < h[b].rc2_tail;
+    }
     check_cuda(cudaMemcpy(d_boxes, h.data(), sizeof(BoxDesc) * nb, cudaMemcpyHostToDevice), "boxes");
     check_cuda(cudaMalloc(&d_done, sizeof(int) * 4), "done");
     check_cuda(cudaMemset(d_done, 0, sizeof(int) * 4), "done");

@@ -429,22 +429,56 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__rest
 }
 
 // ---------------------------------------------------------------------------
-// R11: neighbour list, warp per bin.  The 27 stencil bins are concatenated into one
-// candidate stream (lane = candidate, 32 per round).  Each of up to 32 centres of the bin is
-// tested against the round; the ballot of centre c goes to shared memory, so after the round
-// each centre's lane reads the mask of its hits.  The lanes then write their hits in
-// candidate order, one per iteration of a loop as long as the largest mask.  Work items are
-// 8 bins (one per warp) of a 256-bin unit, taken grid-stride so every SM stays full whatever
-// the number of rebuilding boxes.
+// R11: neighbour list, warp per bin, in two phases per chunk of candidates:
+//   filter  the 27 stencil bins are streamed once (lane = candidate); a candidate is kept
+//           when it lies within the cutoff of the box bounding the bin's centres (the FP32
+//           bound is exact: each axis gap rounds to at most the gap to any centre, and the
+//           squared distance is monotone in the gaps), compacted into shared memory
+//           (x, y, z, j) -- about 3/4 of the candidates, the corners of the stencil drop out
+//   test    lane = kept candidate, loop over the centres: the ballot of centre c is the set of
+//           its hits in the round; a hit's lane writes it straight into c's row at c's count
+//           (held by lane c) plus its rank in the ballot, so rows fill in candidate order
+// A hit is a pair within the cutoff, not the centre itself; on a box with list_reduce also
+// owned by the centre (a local above it, or an upper ghost image) or within rn2_list: the
+// other pairs can enter neither the density sum nor the pair-once force list before the next
+// build.
+// Work items are 8 bins (one per warp) of a 256-bin unit, taken grid-stride so every SM
+// stays full whatever the number of rebuilding boxes.
 // ---------------------------------------------------------------------------
+constexpr int kListChunk = 224;                 // kept candidates per chunk (7 rounds)
+
+__device__ __forceinline__ float warp_min(float v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float warp_max(float v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// hit of this lane for centre c (index cic, count so far base) into c's row
+__device__ __forceinline__ void list_put(int *table, int ncol, int cic, int base, unsigned bal,
+                                         unsigned lt, bool hit, int j)
+{
+    if (hit) {
+        const int p = base + __popc(bal & lt);
+        if (p < ncol)
+            table[(cic & ~31) * ncol + (cic & 31) + (p & 31) * ncol + (p & ~31)] = j;
+    }
+}
+
 __global__ void __launch_bounds__(256, 5) k_rb_list(const BoxDesc *__restrict__ boxes,
                                                  const Unit *__restrict__ units, int nunits,
                                                  int nbox, int *done)
 {
-    __shared__ float4 s_c[8][32];   // centre position (far away in unused slots)
-    __shared__ unsigned s_bal[8][32];  // hit mask of centre c over the round's candidates
+    __shared__ float4 s_c[8][32];                       // centre positions, index in .w
+    __shared__ float4 s_q[8][kListChunk];               // kept candidates: x, y, z, j | upper << 30
     __shared__ int s_bs[8][32], s_cum[8][33];
     const int lane = threadIdx.x & 31, w = threadIdx.x / 32;
+    const unsigned lt = (1u << lane) - 1u;
     const int nitems = nunits * 32;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const Unit U = units[it >> 5];
@@ -455,7 +489,9 @@ __global__ void __launch_bounds__(256, 5) k_rb_list(const BoxDesc *__restrict__ 
         const int s = B.bin_start[b], e = B.bin_start[b + 1];
         if (e == s || B.bin_order[s] >= B.nlocal) continue;  // no locals in this bin
         const float rc2 = B.rc2_tail;
+        const float rn2 = B.list_reduce ? B.rn2_list : rc2;  // with rc2: every pair (full list)
         const int ncol = B.n_col, nlocal = B.nlocal;
+        int *table = B.table;
         const int bx = b % B.mbin[0], by = (b / B.mbin[0]) % B.mbin[1], bz = b / (B.mbin[0] * B.mbin[1]);
         // stencil bins: lane l < 27 takes offset (l%3-1, l/3%3-1, l/9-1)
         int st = 0, sz = 0;
@@ -486,47 +522,62 @@ __global__ void __launch_bounds__(256, 5) k_rb_list(const BoxDesc *__restrict__ 
             const unsigned cm = __ballot_sync(0xffffffffu, is_c);
             if (cm == 0) break;
             const int nc = __popc(cm);
-            s_c[w][lane] = is_c ? B.bpos[pc] : make_float4(3e30f, 3e30f, 3e30f, 0.f);
-            // row of this lane's centre in the locally transposed table
-            int *row = B.table + (ci & ~31) * ncol + (ci & 31);
-            int my_n = 0;
-            // this lane's centre appears in the candidate stream at slot 13 (the own bin)
-            const int q_self = s_cum[w][13] + (pc - s_bs[w][13]);
-            const int ncu = (nc + 3) & ~3;
+            const float4 pc4 = is_c ? B.bpos[pc] : make_float4(0.f, 0.f, 0.f, 0.f);
+            s_c[w][lane] = make_float4(pc4.x, pc4.y, pc4.z, __int_as_float(ci));
+            const float inf = __int_as_float(0x7f800000);
+            const float lox = warp_min(is_c ? pc4.x : inf), hix = warp_max(is_c ? pc4.x : -inf);
+            const float loy = warp_min(is_c ? pc4.y : inf), hiy = warp_max(is_c ? pc4.y : -inf);
+            const float loz = warp_min(is_c ? pc4.z : inf), hiz = warp_max(is_c ? pc4.z : -inf);
+            int my_n = 0;  // lane c: entries of centre c so far
             __syncwarp();
-            for (int q0 = 0; q0 < total; q0 += 32) {
-                const int q = q0 + lane;
-                float4 pj = make_float4(1e30f, 1e30f, 1e30f, 0.f);
-                int j = -1;
-                if (q < total) {
-                    int lo = 0, hi = 27;  // largest slot with s_cum[slot] <= q
-                    while (hi - lo > 1) {
-                        const int mid = (lo + hi) >> 1;
-                        if (s_cum[w][mid] <= q) lo = mid;
-                        else hi = mid;
+            for (int qs = 0; qs < total;) {
+                // filter: fill up to kListChunk kept candidates
+                int nk = 0;
+                for (; qs < total && nk <= kListChunk - 32; qs += 32) {
+                    const int q = qs + lane;
+                    bool keep = false;
+                    float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
+                    int j = 0;
+                    if (q < total) {
+                        int lo = 0, hi = 27;  // largest slot with s_cum[slot] <= q
+                        while (hi - lo > 1) {
+                            const int mid = (lo + hi) >> 1;
+                            if (s_cum[w][mid] <= q) lo = mid;
+                            else hi = mid;
+                        }
+                        const int p = s_bs[w][lo] + (q - s_cum[w][lo]);
+                        pj = B.bpos[p];
+                        j = B.bin_order[p];
+                        const float gx = fmaxf(fmaxf(lox - pj.x, pj.x - hix), 0.f);
+                        const float gy = fmaxf(fmaxf(loy - pj.y, pj.y - hiy), 0.f);
+                        const float gz = fmaxf(fmaxf(loz - pj.z, pj.z - hiz), 0.f);
+                        keep = dist2(gx, gy, gz) <= rc2;
                     }
-                    const int p = s_bs[w][lo] + (q - s_cum[w][lo]);
-                    pj = B.bpos[p];
-                    j = B.bin_order[p];
-                }
-#pragma unroll 4
-                for (int c = 0; c < ncu; ++c) {
-                    const float4 cc = s_c[w][c];
-                    const float r2 = dist2(cc.x - pj.x, cc.y - pj.y, cc.z - pj.z);
-                    const unsigned bal = __ballot_sync(0xffffffffu, r2 <= rc2);
-                    if (lane == 0) s_bal[w][c] = bal;
+                    const unsigned kb = __ballot_sync(0xffffffffu, keep);
+                    const int up = j >= nlocal && (pflags(pj) & kUpperImage) ? 1 << 30 : 0;
+                    if (keep) s_q[w][nk + __popc(kb & lt)] = make_float4(pj.x, pj.y, pj.z, __int_as_float(j | up));
+                    nk += __popc(kb);
                 }
                 __syncwarp();
-                unsigned mine = lane < nc ? s_bal[w][lane] : 0u;
-                if ((unsigned)(q_self - q0) < 32u) mine &= ~(1u << (q_self - q0));  // not itself
-                const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(mine));
-                for (int r = 0; r < rounds; ++r) {
-                    const int src = mine ? __ffs(mine) - 1 : 0;
-                    const int jq = __shfl_sync(0xffffffffu, j, src);
-                    if (mine) {
-                        if (my_n < ncol) row[(my_n & 31) * ncol + (my_n & ~31)] = jq;
-                        ++my_n;
-                        mine &= mine - 1u;
+                // test: lane = kept candidate, one ballot per centre, hits written at once
+                const int R = (nk + 31) >> 5;
+                for (int r = 0; r < R; ++r) {
+                    const int k = (r << 5) + lane;
+                    const bool live = k < nk;
+                    const float4 pj = live ? s_q[w][k] : make_float4(1e30f, 1e30f, 1e30f, 0.f);
+                    // ownership key: a local's index; an upper ghost image above every local,
+                    // a lower one below
+                    const int jw = __float_as_int(pj.w), jv = jw & 0x3fffffff;
+                    const int key = jv < nlocal ? jv : (jw >> 30 ? 0x7fffffff : -1);
+#pragma unroll 4
+                    for (int c = 0; c < nc; ++c) {
+                        const float4 cc = s_c[w][c];
+                        const int cic = __float_as_int(cc.w);
+                        const float r2 = dist2(cc.x - pj.x, cc.y - pj.y, cc.z - pj.z);
+                        const bool hit = r2 <= rc2 && key != cic && (key > cic || r2 <= rn2);
+                        const unsigned bal = __ballot_sync(0xffffffffu, hit);
+                        list_put(table, ncol, cic, __shfl_sync(0xffffffffu, my_n, c), bal, lt, hit, jv);
+                        if (lane == c) my_n += __popc(bal);
                     }
                 }
                 __syncwarp();

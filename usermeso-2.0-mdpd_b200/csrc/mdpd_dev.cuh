@@ -104,6 +104,11 @@ struct BoxDesc {
     int n_col2;
     unsigned long long *facc;  // 3 x nlocal fixed-point force sums (2^-32 units), SoA
     float rc2_force;      // largest force cutoff squared
+    // pair-once boxes without walls keep, of the pairs within the list cutoff, only those the
+    // passes can use before the next build: the owned ones and those within the density cutoff
+    // plus the skin (rn2_list, squared, with a 1e-3 margin over the FP32 rounding of positions)
+    float rn2_list;
+    int list_reduce;      // set by the batch that steps the box
     // ---- rebuild scratch ----
     int *bin_rank;        // Morton rank of each bin (reorder class order)
     int *cls_count, *cls_start, *cls_cursor;  // 2*nbin
