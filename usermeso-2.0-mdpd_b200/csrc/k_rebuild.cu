@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_cls(const BoxDesc *__restr
 // R4 / R10: warp per bucket, order members by (sub key, index) or by index
 // ---------------------------------------------------------------------------
 template <int MODE>  // 0: reorder classes -> perm, 1: bins -> bin_order + bpos
-__global__ void __launch_bounds__(256) k_rb_bucket(const BoxDesc *__restrict__ boxes,
+__global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict__ boxes,
                                                    const Unit *__restrict__ units, int nunits)
 {
     __shared__ unsigned long long s_key[8][kClassMax];
@@ -292,24 +292,34 @@ __global__ void __launch_bounds__(kUnit) k_rb_permute(BoxDesc *__restrict__ boxe
         if (!rebuilding(B)) continue;
         const int k = U.begin + threadIdx.x;
         if (k >= U.end) continue;
-        const int c = B.st->cur, o = 1 - c;
+        const BoxState &S = *B.st;
+        const int c = S.cur, o = 1 - c;
         const int old = B.perm[k];
+        // every load of the particle is issued before the first store (the compiler may not move
+        // a load above a store to a possibly aliased array): one memory round trip
         double x[3], v[3];
         for (int d = 0; d < 3; ++d) {
             x[d] = B.x[c][d][old];
             v[d] = B.v[c][d][old];
+        }
+        const float4 f = B.f[c][old];
+        const int tag = B.tag[c][old], type = B.type[c][old], mask = B.mask[c][old];
+        const float phi = B.phi[c][old];
+        // packed state for the current step (the step counter was advanced by integrate, which
+        // left this step's seed in the box state)
+        const long long step = S.step;
+        const bool sn_cached = S.sn_ok && S.sn_step == step + 1 && S.sn_seed == B.seed;
+        const uint32_t sn = sn_cached ? S.sn_prev : seed_now(B.seed, step);  // box-uniform branch
+        for (int d = 0; d < 3; ++d) {
             B.x[o][d][k] = x[d];
             B.v[o][d][k] = v[d];
             B.xh[d][k] = x[d];
         }
-        B.f[o][k] = B.f[c][old];
-        const int tag = B.tag[c][old], type = B.type[c][old], mask = B.mask[c][old];
+        B.f[o][k] = f;
         B.tag[o][k] = tag;
         B.type[o][k] = type;
         B.mask[o][k] = mask;
-        B.phi[o][k] = B.phi[c][old];
-        // packed state for the current step (the step counter was advanced by integrate)
-        const uint32_t sn = seed_now(B.seed, B.st->step);
+        B.phi[o][k] = phi;
         const float fvx = (float)v[0], fvy = (float)v[1], fvz = (float)v[2];
         B.pos[k] = make_float4((float)(x[0] - B.cen[0]), (float)(x[1] - B.cen[1]),
                                (float)(x[2] - B.cen[2]), pack_w(B, type, mask));
@@ -615,7 +625,7 @@ void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const S
     k_rb_key<<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
     scan<kSelCls>(s, boxes, u.scan_cls, u.nbox, sms);
     k_rb_scatter_cls<<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
-    k_rb_bucket<0><<<g(u.cls.n, 4), 256, 0, s>>>(boxes, u.cls.d, u.cls.n);
+    k_rb_bucket<0><<<g(u.cls.n, 5), 256, 0, s>>>(boxes, u.cls.d, u.cls.n);
     if (c.style == 0)
         k_rb_permute<0><<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done);
     else
@@ -624,7 +634,7 @@ void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const S
     k_rb_ghosts<<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
     scan<kSelBin>(s, boxes, u.scan_bin, u.nbox, sms);
     k_rb_scatter_bins<<<g(u.all.n, 8), kUnit, 0, s>>>(boxes, u.all.d, u.all.n);
-    k_rb_bucket<1><<<g(u.bins.n, 4), 256, 0, s>>>(boxes, u.bins.d, u.bins.n);
+    k_rb_bucket<1><<<g(u.bins.n, 5), 256, 0, s>>>(boxes, u.bins.d, u.bins.n);
     k_rb_list<<<g(u.bins.n * 32, 5), 256, 0, s>>>(boxes, u.bins.d, u.bins.n, u.nbox, done + 1);
 }
 

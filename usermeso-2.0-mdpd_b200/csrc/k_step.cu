@@ -172,10 +172,15 @@ __global__ void __launch_bounds__(kUnit, integrate_blocks(WALL)) k_integrate(Box
             if (ago >= B.delay && ago % B.every == 0) rb = B.check ? moved : 1;
             S->rebuild = rb;
             S->ago = rb ? 0 : ago;
-            S->step += 1;
-            // the next step's seed, once per box instead of once per particle (64 TEA rounds)
-            S->sn = seed_now(B.seed, S->step + 1);
-            S->sn_step = S->step + 1;
+            // this step's seed (for a rebuild's pack) and the next step's, once per box instead
+            // of once per particle (64 TEA rounds)
+            const long long s1 = S->step + 1;
+            const uint32_t used =
+                S->sn_ok && S->sn_step == s1 && S->sn_seed == B.seed ? S->sn : seed_now(B.seed, s1);
+            S->step = s1;
+            S->sn_prev = used;
+            S->sn = seed_now(B.seed, s1 + 1);
+            S->sn_step = s1 + 1;
             S->sn_seed = B.seed;
             S->sn_ok = 1;
             any |= rb;

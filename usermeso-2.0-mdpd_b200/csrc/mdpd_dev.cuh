@@ -49,11 +49,12 @@ struct BoxState {
     long long nbuild;
     int cur;               // live copy of the double-buffered arrays
     int pad;
-    // seed_now(sn_seed, sn_step), computed once per box by the integrate pass of the step
-    // before (valid when sn_ok; a host-written state has sn_ok = 0)
+    // seed_now(sn_seed, sn_step) and seed_now(sn_seed, sn_step - 1), computed once per box by
+    // the integrate pass of the step before (valid when sn_ok; a host-written state has sn_ok = 0)
     long long sn_step;
     uint32_t sn_seed, sn;
-    int sn_ok, pad2;
+    int sn_ok;
+    uint32_t sn_prev;
 };
 
 struct BoxDesc {
