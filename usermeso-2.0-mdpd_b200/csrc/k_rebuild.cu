@@ -240,6 +240,11 @@ __global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict_
             if (n == 0) continue;
             const int s = start[b];
             __syncwarp();
+            if (MODE == 1 && arr[s + n - 1] < B.nlocal) {
+                // locals only: already in index order, bpos written by the scatter
+                if (lane == 0) cnt[b] = 0;
+                continue;
+            }
             if (n > kClassMax) {
                 if (lane == 0) {
                     atomicOr(&B.st->status, kErrBucketOverflow);
@@ -422,7 +427,11 @@ __global__ void __launch_bounds__(kUnit) k_rb_ghosts(const BoxDesc *__restrict__
 }
 
 // ---------------------------------------------------------------------------
-// R9: scatter locals+ghosts into bins
+// R9: scatter locals+ghosts into bins.  A local's place needs no atomics: the reorder sort
+// left a bin's bulk particles, then its border particles, as two runs of consecutive indices,
+// so its rank in the bin (in index order) follows from the class starts; its packed position
+// goes to bpos as well.  Ghost images take atomic slots after the bin's locals, and the bin
+// sort puts them in index order.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__restrict__ boxes,
                                                            const Unit *__restrict__ units, int nunits)
@@ -432,8 +441,20 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__rest
         const BoxDesc &B = boxes[U.box];
         if (!rebuilding(B)) continue;
         const int i = U.begin + threadIdx.x;
-        if (i >= U.end || i >= B.nlocal + min(B.st->nghost, B.ghost_cap)) continue;
-        const int p = atomicAdd(&B.bin_cursor[B.bin_of[i]], 1);
+        const int nl = B.nlocal;
+        if (i >= U.end || i >= nl + min(B.st->nghost, B.ghost_cap)) continue;
+        const int bin = B.bin_of[i];
+        const int rk = B.bin_rank[bin];
+        const int b0 = B.cls_start[rk], b1 = B.cls_start[rk + 1];  // the bin's bulk run
+        const int e0 = B.cls_start[B.nbin + rk];                     // its border run
+        int p;
+        if (i < nl) {
+            p = B.bin_start[bin] + (i < B.st->n_bulk ? i - b0 : (b1 - b0) + (i - e0));
+            B.bpos[p] = B.pos[i];
+        } else {
+            const int nloc = (b1 - b0) + (B.cls_start[B.nbin + rk + 1] - e0);
+            p = atomicAdd(&B.bin_cursor[bin], 1) + nloc;
+        }
         B.bin_order[p] = i;
     }
 }
@@ -539,6 +560,7 @@ __global__ void __launch_bounds__(256, 5) k_rb_list(const BoxDesc *__restrict__ 
             const float loy = warp_min(is_c ? pc4.y : inf), hiy = warp_max(is_c ? pc4.y : -inf);
             const float loz = warp_min(is_c ? pc4.z : inf), hiz = warp_max(is_c ? pc4.z : -inf);
             int my_n = 0;  // lane c: entries of centre c so far
+            int slot = 0;  // stencil slot of this lane's stream position (only grows)
             __syncwarp();
             for (int qs = 0; qs < total;) {
                 // filter: fill up to kListChunk kept candidates
@@ -549,13 +571,9 @@ __global__ void __launch_bounds__(256, 5) k_rb_list(const BoxDesc *__restrict__ 
                     float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
                     int j = 0;
                     if (q < total) {
-                        int lo = 0, hi = 27;  // largest slot with s_cum[slot] <= q
-                        while (hi - lo > 1) {
-                            const int mid = (lo + hi) >> 1;
-                            if (s_cum[w][mid] <= q) lo = mid;
-                            else hi = mid;
-                        }
-                        const int p = s_bs[w][lo] + (q - s_cum[w][lo]);
+                        // largest slot with s_cum[slot] <= q (s_cum[27] = total > q ends the walk)
+                        while (s_cum[w][slot + 1] <= q) ++slot;
+                        const int p = s_bs[w][slot] + (q - s_cum[w][slot]);
                         pj = B.bpos[p];
                         j = B.bin_order[p];
                         const float gx = fmaxf(fmaxf(lox - pj.x, pj.x - hix), 0.f);
