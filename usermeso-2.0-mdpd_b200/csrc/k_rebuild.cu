@@ -38,8 +38,10 @@ __global__ void __launch_bounds__(kUnit) k_rb_key(const BoxDesc *__restrict__ bo
         const int c = B.st->cur;
         uint32_t bid[3], sub[3];
         bool border = false;
+        double xs[3];  // all three loads before the first store (no round trip per axis)
+        for (int d = 0; d < 3; ++d) xs[d] = B.x[c][d][i];
         for (int d = 0; d < 3; ++d) {
-            double x = B.x[c][d][i];
+            double x = xs[d];
             if (x < B.lo[d]) x += B.prd[d];
             if (x >= B.hi[d]) {
                 x -= B.prd[d];
