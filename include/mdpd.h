@@ -6,7 +6,7 @@
  *   PairStyle(mdpd/meso, MesoPairMDPD)        src/USER-MESO/pair_mdpd_meso.h:3
  *   PairStyle(dpd/meso, MesoPairDPD)          src/USER-MESO/pair_dpd_meso.h:3
  *   AtomStyle(mdpd/atomic/meso, ...)          src/USER-MESO/atom_vec_mdpd_atomic_meso.h:3
- *   FixStyle(nve/meso / aboundary/rho/meso / addforce/meso / density/meso, ...)
+ *   FixStyle(nve/meso / aboundary/rho/meso / aboundary/meso / addforce/meso / density/meso, ...)
  *   IntegrateStyle(mvv/meso, ModifiedVerlet)  src/USER-MESO/mvv_meso.h:3-4
  *   Input::file/one -> Force::create_pair / Modify::add_fix / Run::command (src/run.cpp:170-178)
  * A caller replaces that chain by these entry points.  Every call returns an MDPD_* status;

@@ -450,6 +450,60 @@ void orc_reduce_rows(int nlocal, int ncol, const int32_t *count, const int32_t *
     }
 }
 
+/* fix aboundary/meso at the end of a step (gpu_aboundary_v2, fix_aboundary_meso.cu:186-281):
+ * a particle of the mobile group is projected half a kick and one drift ahead (v + dt/2 f,
+ * x + dt v, unit mass as the reference writes it); the Gaussian density of the wall particles
+ * among its row's core entries (the first count_core[i], core entries first as the reference
+ * joins them) is summed at that point; above rho0/2 the parts of v and f along the direction
+ * into the wall (minus the normalised density gradient) are removed twice over.  FP32 as the
+ * reference; its contracted forms are written as fmaf.  v and f (the total force) in place. */
+static float orc_dot3f(float ax, float ay, float az, float bx, float by, float bz)
+{
+    return fmaf(az, bz, fmaf(ax, bx, ay * by));
+}
+
+void orc_aboundary_meso(int nlocal, const float *pos4, const int32_t *mask_all, const int32_t *count_core,
+                        const int32_t *table, int ncol, int mobile_bit, int wall_bit, double rho0, double sigma,
+                        double dt, double *vx, double *vy, double *vz, double *fx, double *fy, double *fz)
+{
+    const float sg = (float)sigma, r0 = (float)rho0, dtf = (float)dt;
+    const float nf = (float)(1.0 / sqrt(pow(2 * M_PI, 3.0) * pow(sigma, 3.0))); /* :275 */
+    const float hs = (float)(0.5 * (double)dtf);
+    const float ex = -0.5f / sg;
+    for (int i = 0; i < nlocal; ++i) {
+        if (!(mask_all[i] & mobile_bit)) continue;
+        const float v0x = (float)vx[i], v0y = (float)vy[i], v0z = (float)vz[i];
+        const float f0x = (float)fx[i], f0y = (float)fy[i], f0z = (float)fz[i];
+        const float px = fmaf(hs, f0x, v0x), py = fmaf(hs, f0y, v0y), pz = fmaf(hs, f0z, v0z);
+        const float cx = fmaf(dtf, px, pos4[4 * i]), cy = fmaf(dtf, py, pos4[4 * i + 1]),
+                    cz = fmaf(dtf, pz, pos4[4 * i + 2]);
+        float rho = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+        for (int k = 0; k < count_core[i]; ++k) {
+            const int j = table[(size_t)i * ncol + k];
+            if (!(mask_all[j] & wall_bit)) continue;
+            const float dx = cx - pos4[4 * j], dy = cy - pos4[4 * j + 1], dz = cz - pos4[4 * j + 2];
+            const float w = nf * expf(ex * orc_dr2f(dx, dy, dz));
+            rho += w;
+            const float ws = w / sg;
+            gx = fmaf(dx, ws, gx);
+            gy = fmaf(dy, ws, gy);
+            gz = fmaf(dz, ws, gz);
+        }
+        if (rho > 0.5f * r0) {
+            const float inv = 1.0f / sqrtf(orc_dot3f(gx, gy, gz, gx, gy, gz));
+            const float ex_ = -(gx * inv), ey_ = -(gy * inv), ez_ = -(gz * inv);
+            const float vd = fmaxf(0.f, orc_dot3f(v0x, v0y, v0z, ex_, ey_, ez_));
+            const float fd = fmaxf(0.f, orc_dot3f(f0x, f0y, f0z, ex_, ey_, ez_));
+            vx[i] -= (double)(2.f * vd * ex_);
+            vy[i] -= (double)(2.f * vd * ey_);
+            vz[i] -= (double)(2.f * vd * ez_);
+            fx[i] -= (double)(2.f * fd * ex_);
+            fy[i] -= (double)(2.f * fd * ey_);
+            fz[i] -= (double)(2.f * fd * ez_);
+        }
+    }
+}
+
 typedef struct { uint64_t key; int bin; } stencil_t;
 
 static int stencil_cmp(const void *a, const void *b)

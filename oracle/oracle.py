@@ -191,6 +191,21 @@ def reduce_rows(count, table, pos4, gimg, rn2):
     return oc, ot
 
 
+def aboundary_meso(pos4, mask_all, count_core, table, mobile_bit, wall_bit, rho0, sigma, dt, v, f):
+    """fix aboundary/meso at the end of a step: returns (v, f) after the wall reflection."""
+    n, ncol = table.shape
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    mask_all = np.ascontiguousarray(mask_all, np.int32)
+    cc = np.ascontiguousarray(count_core, np.int32)
+    table = np.ascontiguousarray(table, np.int32)
+    vv = [np.ascontiguousarray(v[:, d], np.float64).copy() for d in range(3)]
+    ff = [np.ascontiguousarray(f[:, d], np.float64).copy() for d in range(3)]
+    lib().orc_aboundary_meso(n, P(pos4, C.c_float), P(mask_all, C.c_int32), P(cc, C.c_int32), P(table, C.c_int32),
+                             ncol, mobile_bit, wall_bit, C.c_double(rho0), C.c_double(sigma), C.c_double(dt),
+                             *[P(a, C.c_double) for a in vv + ff])
+    return np.stack(vv, 1), np.stack(ff, 1)
+
+
 def density(pos4, count, table, mask, groupbit, cut_rho, mass_type):
     n = len(count)
     ncol = table.shape[1]

@@ -62,6 +62,19 @@ neigh_modify every 1 delay 0 check yes
     with pytest.raises(mdpd.MdpdError) as e:
         L.command("fix BC all aboundary/rho/meso")
     assert "not set properly" in str(e.value)
+    # fix aboundary/meso: the reference's errors (fix_aboundary_meso.cu:46-77)
+    L.command("group fluid type 1")
+    with pytest.raises(mdpd.MdpdError) as e:
+        L.command("fix W fluid aboundary/meso wall nosuch rc 1.0 rho 8.0")
+    assert "Undefined wall group id in fix aboundary/meso" in str(e.value)
+    with pytest.raises(mdpd.MdpdError) as e:
+        L.command("fix W fluid aboundary/meso wall all rc 1.0")
+    assert "Fix aboundary/meso usage: aboundary/meso <wall groupid> <rc double> <rho double>" in str(e.value)
+    L.command("fix W fluid aboundary/meso wall all rho 8.0 sigma 0.1 rc 1.0 frac 0.3")  # keywords in any order
+    assert "overlapped" not in L.log  # the reference compares the two groups' bits
+    L.command("fix W fluid aboundary/meso wall fluid rho 8.0 rc 1.0")
+    assert "mobile and wall group overlapped" in L.log
+    L.command("unfix W")
     with pytest.raises(mdpd.MdpdError) as e:
         L.command("frobnicate 1 2 3")
     assert e.value.code == mdpd.ERR_PARSE

@@ -244,6 +244,13 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
         B.rn2_list = (float)(rn * rn);
         B.list_reduce = 0;
     }
+    B.rc2_core = (float)std::pow(g.cutneighmax - s.skin, 2.0);  // neigh_build_meso.cu:316-317
+    B.ab_mobile_bit = s.ab_mobile_bit;
+    B.ab_wall_bit = s.ab_wall_bit;
+    B.ab_rho0 = (float)s.ab_rho0;
+    B.ab_sigma = (float)s.ab_sigma;
+    // 1 / sqrt((2 pi)^3 sigma^3), the Gaussian's normalisation (fix_aboundary_meso.cu:275)
+    B.ab_nfactor = s.ab_mobile_bit ? (float)(1.0 / std::sqrt(std::pow(2 * M_PI, 3.0) * std::pow(s.ab_sigma, 3.0))) : 0.f;
     B.n_col2 = g.n_col2;
     nbin = B.nbin = g.mbin[0] * g.mbin[1] * g.mbin[2];
     B.nlocal = n;
@@ -460,7 +467,8 @@ Batch::Batch(std::vector<Box *> boxes, const StepConfig &c) : cfg(c), boxes_(std
     for (int b = 0; b < nb; ++b) {
         h[b] = boxes_[b]->desc;
         // the reduced list serves the pair-once passes only (the wall fix reads the full list)
-        h[b].list_reduce = cfg.half && !cfg.wall && !h[b].wall_fix && h[b].rn2_list < h[b].rc2_tail;
+        h[b].list_reduce = cfg.half && !cfg.wall && !h[b].wall_fix && !h[b].ab_mobile_bit &&
+                           h[b].rn2_list < h[b].rc2_tail;
     }
     check_cuda(cudaMemcpy(d_boxes, h.data(), sizeof(BoxDesc) * nb, cudaMemcpyHostToDevice), "boxes");
     check_cuda(cudaMalloc(&d_done, sizeof(int) * 4), "done");
@@ -551,6 +559,7 @@ void Batch::capture(int ev)
     cudaStreamDestroy(s2);
     if (cfg.style == 0) launch_density(stream_, d_boxes, units, cfg);
     launch_force(stream_, d_boxes, units, cfg, ev, 1);
+    if (cfg.aboundary) launch_aboundary_meso(stream_, d_boxes, units);  // end of step, before output
     if (ev) launch_thermo(stream_, d_boxes, units, d_thermo, d_done + 2);
     check_cuda(cudaStreamEndCapture(stream_, &tmp), "end capture");
     check_cuda(cudaGraphInstantiate(&graph_[ev], g, 0), "instantiate");
@@ -642,6 +651,7 @@ void Batch::profile(long long nsteps, double out[5])
         if (cfg.style == 0) launch_density(stream_, d_boxes, units, cfg);
         cudaEventRecord(ev[3], stream_);
         launch_force(stream_, d_boxes, units, cfg, 0, 1);
+        if (cfg.aboundary) launch_aboundary_meso(stream_, d_boxes, units);
         cudaEventRecord(ev[4], stream_);
         check_cuda(cudaEventSynchronize(ev[4]), "profile");
         for (int q = 0; q < 4; ++q) {

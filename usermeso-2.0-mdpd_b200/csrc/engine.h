@@ -36,6 +36,9 @@ struct Spec {
     int arb_bc = 0, mobile_bit = 0, wall_bit = 0;  // pair_style ... fluid_group wall_group
     int wall_fix = 0;                              // aboundary wall/mobile given
     double cut_phi = 0, rho_wall = 0, phi_c = 0;
+    // fix aboundary/meso (fix_aboundary_meso.cu:31-82): group, wall group, rho, sigma
+    int ab_mobile_bit = 0, ab_wall_bit = 0;
+    double ab_rho0 = 0, ab_sigma = 0;
     int exact_rng = 0;
     double ghost_factor = 1.0;   // ghost capacity multiplier
 };

@@ -227,6 +227,101 @@ void launch_force_rebuild_flag(cudaStream_t s, BoxDesc *boxes, int nbox, int val
 }
 
 // ---------------------------------------------------------------------------
+// fix aboundary/meso (fix_aboundary_meso.cu:186-281, gpu_aboundary_v2 at end_of_step): for a
+// particle of the fix's group, project it half a kick and one drift ahead, sum a Gaussian
+// density of the wall particles among its list's core entries (the pairs within the cutoff at
+// the build), and where that density passes rho0/2 remove the parts of v and f pointing into
+// the wall.  FP32 as the reference, with its contractions spelled out.  The core entries are
+// recovered from the build positions (xh, packed exactly as the build packed them) with the
+// list build's FP32 test against the core cutoff.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float3 packed_at_build(const BoxDesc &B, int j)
+{
+    int s = j, code = 13;
+    if (j >= B.nlocal) {
+        s = B.gsrc[j - B.nlocal];
+        code = B.gimg[j - B.nlocal];
+    }
+    return make_float3((float)(B.xh[0][s] + (code % 3 - 1) * B.prd[0] - B.cen[0]),
+                       (float)(B.xh[1][s] + ((code / 3) % 3 - 1) * B.prd[1] - B.cen[1]),
+                       (float)(B.xh[2][s] + (code / 9 - 1) * B.prd[2] - B.cen[2]));
+}
+
+// a.x*b.x + a.y*b.y + a.z*b.z as nvcc contracts it (the form of dist2)
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz)
+{
+    return __fmaf_rn(az, bz, __fmaf_rn(ax, bx, __fmul_rn(ay, by)));
+}
+
+__global__ void __launch_bounds__(kUnit) k_aboundary_meso(BoxDesc *__restrict__ boxes,
+                                                          const Unit *__restrict__ units, int nunits)
+{
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const Unit U = units[u];
+        const BoxDesc &B = boxes[U.box];
+        if (!B.ab_mobile_bit) continue;
+        const int i = U.begin + threadIdx.x;
+        if (i >= U.end) continue;
+        const int c = B.st->cur;
+        const int m = B.mask[c][i];
+        if (!(m & B.ab_mobile_bit)) continue;
+        const float dt = (float)B.dtv;
+        const float hs = (float)(0.5 * (double)dt);
+        const bool body = m & B.body_bit;
+        const float4 fp = B.f[c][i];
+        // the total force (pair + fix addforce/meso), as the reference's f holds it
+        const double fx = (double)fp.x + (body ? B.body[0] : 0.0), fy = (double)fp.y + (body ? B.body[1] : 0.0),
+                     fz = (double)fp.z + (body ? B.body[2] : 0.0);
+        const double vx = B.v[c][0][i], vy = B.v[c][1][i], vz = B.v[c][2][i];
+        const float3 v0 = make_float3((float)vx, (float)vy, (float)vz);
+        const float3 f0 = make_float3((float)fx, (float)fy, (float)fz);
+        const float4 x0 = B.pos[i];
+        const float3 vp = make_float3(__fmaf_rn(hs, f0.x, v0.x), __fmaf_rn(hs, f0.y, v0.y), __fmaf_rn(hs, f0.z, v0.z));
+        const float3 c1 = make_float3(__fmaf_rn(dt, vp.x, x0.x), __fmaf_rn(dt, vp.y, x0.y), __fmaf_rn(dt, vp.z, x0.z));
+        const float3 bi = packed_at_build(B, i);
+        const float sig = B.ab_sigma, rc2 = B.rc2_core, nf = B.ab_nfactor;
+        const float ex = __fdiv_rn(-0.5f, sig);
+        float rho_w = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+        const int n = B.count[i];
+        for (int k = 0; k < n; ++k) {
+            const int j = B.table[list_addr(i, k, B.n_col)];
+            const int mj = j < B.nlocal ? B.mask[c][j] : B.mask[c][B.gsrc[j - B.nlocal]];
+            if (!(mj & B.ab_wall_bit)) continue;
+            const float3 bj = packed_at_build(B, j);
+            if (!(dist2(bi.x - bj.x, bi.y - bj.y, bi.z - bj.z) <= rc2)) continue;  // not a core entry
+            const float4 c2 = B.pos[j];
+            const float dx = c1.x - c2.x, dy = c1.y - c2.y, dz = c1.z - c2.z;
+            const float rsq = dist2(dx, dy, dz);
+            const float w = __fmul_rn(nf, expf(__fmul_rn(ex, rsq)));
+            rho_w += w;
+            const float ws = __fdiv_rn(w, sig);
+            gx = __fmaf_rn(dx, ws, gx);
+            gy = __fmaf_rn(dy, ws, gy);
+            gz = __fmaf_rn(dz, ws, gz);
+        }
+        if (rho_w > 0.5f * B.ab_rho0) {
+            const float inv = rsqrtf(dot3(gx, gy, gz, gx, gy, gz));
+            const float ex_ = -(gx * inv), ey_ = -(gy * inv), ez_ = -(gz * inv);  // e = -normalize(grad)
+            const float vd = fmaxf(0.f, dot3(v0.x, v0.y, v0.z, ex_, ey_, ez_));
+            const float fd = fmaxf(0.f, dot3(f0.x, f0.y, f0.z, ex_, ey_, ez_));
+            B.v[c][0][i] = vx - (double)(2.f * vd * ex_);
+            B.v[c][1][i] = vy - (double)(2.f * vd * ey_);
+            B.v[c][2][i] = vz - (double)(2.f * vd * ez_);
+            // f keeps the pair force; the body force is added again by the kicks
+            B.f[c][i] = make_float4((float)(fx - (double)(2.f * fd * ex_) - (body ? B.body[0] : 0.0)),
+                                    (float)(fy - (double)(2.f * fd * ey_) - (body ? B.body[1] : 0.0)),
+                                    (float)(fz - (double)(2.f * fd * ez_) - (body ? B.body[2] : 0.0)), fp.w);
+        }
+    }
+}
+
+void launch_aboundary_meso(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u)
+{
+    if (u.local.n <= 0) return;
+    k_aboundary_meso<<<u.local.n, kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
+}
+
+// ---------------------------------------------------------------------------
 // density pass: rho_i = m_i * 15/(2 pi h^5) * sum_{r<h} (h - r)^2 over the list.
 // TPP threads per particle split the list and combine with shuffles.
 // ---------------------------------------------------------------------------

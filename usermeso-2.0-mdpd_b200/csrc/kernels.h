@@ -36,6 +36,7 @@ struct StepConfig {
     int half = 0;          // mdpd without wall coupling: each pair evaluated once (k_pair.cu)
     int half_enabled = 1;  // allow the half-list passes (set per batch from the boxes)
     int gather = 6;        // pair-once density pass: neighbour positions in flight per lane (4, 6, 8)
+    int aboundary = 0;     // fix aboundary/meso at the end of each step
     int sms = 148;
 };
 
@@ -53,6 +54,7 @@ void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const S
 void launch_density(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c);
 void launch_force(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev,
                   int kick);
+void launch_aboundary_meso(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u);
 void launch_density_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c);
 void launch_force_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev, int kick);
 // AoS x[3n] (and v[3n], or zero when null) -> components x[d], xh[d], v[d]; tags 1..n, type 1

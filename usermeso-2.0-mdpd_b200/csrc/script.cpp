@@ -721,6 +721,30 @@ void Script::command(const std::string &raw)
                 spec_.mobile_bit = mobile;
             }
             rho_fix_ = id;
+        } else if (style == "aboundary/meso") {
+            // FixArbitraryBoundary ctor (fix_aboundary_meso.cu:31-82): keywords anywhere in the line
+            int wall = 0;
+            double rc = 0, rho0 = 0, sigma = 0;
+            for (int k = 1; k <= narg; ++k) {
+                if (a[k] == "wall" && k < narg) {
+                    auto g = groups_.find(a[++k]);
+                    if (g == groups_.end()) parse_error("<MESO> Undefined wall group id in fix aboundary/meso");
+                    wall = 1 << g->second;
+                    if (gb & wall) log += "WARNING: <MESO> fix aboundary/meso mobile and wall group overlapped\n";
+                }
+                if (a[k] == "rc" && k < narg) rc = num(a[++k]);
+                else if (a[k] == "rho" && k < narg) rho0 = num(a[++k]);
+                else if (a[k] == "sigma" && k < narg) sigma = num(a[++k]);
+                else if (a[k] == "frac" && k < narg) ++k;  // read and unused by the reference
+            }
+            if (wall == 0 || rc == 0 || rho0 == 0)
+                parse_error("<MESO> Fix aboundary/meso usage: " + style +
+                            " <wall groupid> <rc double> <rho double> [sigma double]");
+            spec_.ab_mobile_bit = gb;
+            spec_.ab_wall_bit = wall;
+            spec_.ab_rho0 = rho0;
+            spec_.ab_sigma = sigma == 0 ? rc * rc / 4.0 / M_PI : sigma;
+            ab_fix_ = id;
         } else if (style == "addforce/meso") {
             // fix ID group addforce/meso fx fy fz; extra words are ignored (fix_addforce_meso.cu:37-48)
             if (narg < 6) parse_error("Illegal fix addforce/meso command");
@@ -751,6 +775,7 @@ void Script::command(const std::string &raw)
     } else if (c == "unfix") {
         if (narg != 1) parse_error("Illegal unfix command");
         if (a[1] == nve_fix_) spec_.nve_bit = 0, nve_fix_.clear();
+        if (a[1] == ab_fix_) spec_.ab_mobile_bit = spec_.ab_wall_bit = 0, ab_fix_.clear();
         for (size_t k = 0; k < dens_.size(); ++k)
             if (dens_[k].id == a[1]) {
                 if (dens_[k].d_counts) cudaFree(dens_[k].d_counts);
@@ -864,6 +889,7 @@ void Script::ensure_device()
     cfg.style = spec_.style;
     cfg.exact_rng = spec_.exact_rng;
     cfg.wall = spec_.wall_fix;
+    cfg.aboundary = spec_.ab_mobile_bit != 0;
     cfg.wall_coupling = spec_.arb_bc;
     box_.reset(new Box(spec_, parts_, cfg.sms));
     // device step counter starts at the script's current step

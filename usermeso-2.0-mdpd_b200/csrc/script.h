@@ -75,7 +75,7 @@ private:
     double lattice_a_ = 1.0;
     int lattice_fcc_ = 0;
     int pair_set_ = 0;
-    std::string nve_fix_, rho_fix_;
+    std::string nve_fix_, rho_fix_, ab_fix_;
     std::vector<DensityFix> dens_;
     std::vector<DumpSpec> dumps_;
     std::unique_ptr<Box> box_;
