@@ -222,7 +222,8 @@ def main():
         barrier()
     r1 = b.rebuild_steps()
     value, t_max = aggregate(ntot * args.steps, ms * args.steps / 1e3, world)
-    gpu_launches = 3 * args.steps + 17 * (r1 - r0)
+    # a pair-once mDPD step: integrate, density, force, finalize; a rebuilding step adds 17
+    gpu_launches = 4 * args.steps + 17 * (r1 - r0)
     eq_states = [b.state(k) for k in range(len(cfg))] if not args.no_extras else None
     b.close()
 
