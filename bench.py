@@ -268,7 +268,7 @@ def main():
         temps = []
         for _ in range(args.steps):
             be.step(1)
-            temps.append(be.thermo(0).temp)  # the step's result, read on the host
+            temps.append([t.temp for t in be.thermo_all()])  # the step's result: every box's thermo
         t2 = time.perf_counter()
         for k in range(len(cfg)):
             be.state(k, xout[k], vout[k])
@@ -280,9 +280,11 @@ def main():
         all_state_bytes, _ = aggregate(state_bytes, 1.0, world)  # summed over ranks
         line["e2e"] = {"value": e2e_value, "unit": "particle-steps/s",
                        "h2d_bytes_per_step": int(all_state_bytes / args.steps),
-                       "d2h_bytes_per_step": int(all_state_bytes / args.steps + world * ctypes.sizeof(mdpd.Thermo)),
+                       "d2h_bytes_per_step": int(all_state_bytes / args.steps +
+                                                 world * len(cfg) * ctypes.sizeof(mdpd.Thermo)),
                        "note": "wall clock of: create of all 256 boxes from pinned host x, v; setup; K steps, "
-                               "each followed by a thermo read; full state download into pinned host arrays",
+                               "each followed by a read of every box's thermo; full state download into "
+                               "pinned host arrays",
                        "split": split}
         del temps, xin, vin, xout, vout
 

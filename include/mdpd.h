@@ -125,6 +125,10 @@ int mdpd_batch_create(mdpd_batch_t **b, const mdpd_box_spec *specs, int32_t nbox
 int mdpd_batch_setup(mdpd_batch_t *b);
 int mdpd_batch_step(mdpd_batch_t *b, int64_t nsteps);
 int mdpd_batch_thermo(mdpd_batch_t *b, int32_t box, mdpd_thermo_t *out);
+/* every box's thermo in one pass (out[nbox], batch order; nbox must equal the batch's): the
+ * per-box compute temp/pressure/pe/meso results (compute_temp_meso.cu:58-101,
+ * compute_pressure_meso.cu:98-150) that mdpd_batch_thermo returns one at a time */
+int mdpd_batch_thermo_all(mdpd_batch_t *b, mdpd_thermo_t *out, int32_t nbox);
 int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int64_t n);
 /* project autotuner: times the candidate shapes of the pair passes on this batch (13 real steps
  * each, so the boxes advance) and keeps the fastest. Pair-once mDPD batches: *shape_density =

@@ -41,6 +41,12 @@ def test_batch_equals_alone_bitwise():
         xb, vb = b.state(k)
         assert np.array_equal(xa, xb) and np.array_equal(va, vb), k
         assert b.thermo(k).nbuild == ta.nbuild
+    # every box's thermo in one pass equals the per-box calls (same fixed-order FP64 sums)
+    every = b.thermo_all()
+    for k in range(len(sp)):
+        one = b.thermo(k)
+        assert (every[k].step, every[k].natoms, every[k].nbuild) == (one.step, one.natoms, one.nbuild)
+        assert (every[k].temp, every[k].pe, every[k].press) == (one.temp, one.pe, one.press)
     b.close()
 
 

@@ -484,6 +484,16 @@ int mdpd_batch_thermo(mdpd_batch_t *b, int32_t box, mdpd_thermo_t *out)
     });
 }
 
+int mdpd_batch_thermo_all(mdpd_batch_t *b, mdpd_thermo_t *out, int32_t nbox)
+{
+    if (!b || !out || nbox != (int32_t)b->boxes.size()) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        std::vector<Thermo> t;
+        b->batch->thermo(t);
+        for (int k = 0; k < nbox; ++k) fill_thermo(t[k], out + k);
+    });
+}
+
 int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int64_t n)
 {
     if (!b || box < 0 || box >= (int)b->boxes.size()) return MDPD_ERR_ARG;

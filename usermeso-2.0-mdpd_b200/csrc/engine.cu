@@ -2,6 +2,8 @@
 // IF(rebuild){...} -> density -> force), setup and thermo.
 #include "engine.h"
 
+#include <array>
+#include <map>
 #include <mutex>
 
 #include <algorithm>
@@ -116,6 +118,27 @@ static cudaMemPool_t box_pool()
         check_cuda(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep), "memory pool");
     }
     return pools[dev];
+}
+
+// Morton rank of each bin of an mbin[0] x mbin[1] x mbin[2] grid (bins in x-major order), one
+// sort per grid shape for the life of the process: a batch of boxes repeats few shapes
+static const std::vector<int> &morton_ranks(const int mbin[3])
+{
+    static std::mutex mu;
+    static std::map<std::array<int, 3>, std::vector<int>> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    std::vector<int> &rank = cache[{mbin[0], mbin[1], mbin[2]}];
+    if (rank.empty()) {
+        const int nbin = mbin[0] * mbin[1] * mbin[2];
+        std::vector<std::pair<uint64_t, int>> codes(nbin);
+        for (int z = 0, b = 0; z < mbin[2]; ++z)
+            for (int y = 0; y < mbin[1]; ++y)
+                for (int x = 0; x < mbin[0]; ++x, ++b) codes[b] = {morton3(x, y, z), b};
+        std::sort(codes.begin(), codes.end());
+        rank.resize(nbin);
+        for (int r = 0; r < nbin; ++r) rank[codes[r].second] = r;
+    }
+    return rank;
 }
 
 template <class T> T *Box::alloc(size_t count)
@@ -334,13 +357,7 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
 
     // Morton rank of every bin: reorder buckets are visited in Morton order of their bin
     {
-        std::vector<std::pair<uint64_t, int>> codes(nbin);
-        for (int z = 0, b = 0; z < g.mbin[2]; ++z)
-            for (int y = 0; y < g.mbin[1]; ++y)
-                for (int x = 0; x < g.mbin[0]; ++x, ++b) codes[b] = {morton3(x, y, z), b};
-        std::sort(codes.begin(), codes.end());
-        std::vector<int> rank(nbin);
-        for (int r = 0; r < nbin; ++r) rank[codes[r].second] = r;
+        const std::vector<int> &rank = morton_ranks(g.mbin);
         check_cuda(cudaMemcpy(B.bin_rank, rank.data(), sizeof(int) * nbin, cudaMemcpyHostToDevice), "upload");
     }
     // initial state into buffer 0: the caller's AoS x and v go to the list table's space (unused

@@ -313,6 +313,12 @@ class Batch:
         self._check(lib().mdpd_batch_thermo(self.h, box, C.byref(t)))
         return t
 
+    def thermo_all(self):
+        """every box's Thermo, batch order, from one pass"""
+        t = (Thermo * len(self.n))()
+        self._check(lib().mdpd_batch_thermo_all(self.h, t, len(self.n)))
+        return list(t)
+
     def state(self, box, x=None, v=None):
         """Positions and velocities of one box in tag order; x, v: optional preallocated
         C-contiguous float64 (n, 3) arrays to fill (pinned ones make the copy a direct DMA)."""
