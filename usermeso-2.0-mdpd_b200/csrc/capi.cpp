@@ -431,17 +431,24 @@ int mdpd_batch_create(mdpd_batch_t **out, const mdpd_box_spec *specs, int32_t nb
         cfg.style = specs[0].style;
         cfg.exact_rng = specs[0].exact_rng;
         std::vector<Box *> raw;
-        for (int k = 0; k < nbox; ++k) {
-            if (specs[k].style != cfg.style) throw std::runtime_error("ARG: a batch holds boxes of one pair style");
-            Spec s;
-            Particles p;
-            spec_from_box(specs[k], s, p);
-            if (specs[k].x)  // the caller's arrays go to the device directly
-                b->boxes.emplace_back(new Box(s, specs[k].n, specs[k].x, specs[k].v, nullptr, nullptr, nullptr, cfg.sms));
-            else
-                b->boxes.emplace_back(new Box(s, p, cfg.sms));
-            raw.push_back(b->boxes.back().get());
+        try {
+            for (int k = 0; k < nbox; ++k) {
+                if (specs[k].style != cfg.style) throw std::runtime_error("ARG: a batch holds boxes of one pair style");
+                Spec s;
+                Particles p;
+                spec_from_box(specs[k], s, p);
+                if (specs[k].x)  // the caller's arrays go to the device directly, the copies queued
+                    b->boxes.emplace_back(
+                        new Box(s, specs[k].n, specs[k].x, specs[k].v, nullptr, nullptr, nullptr, cfg.sms, false));
+                else
+                    b->boxes.emplace_back(new Box(s, p, cfg.sms));
+                raw.push_back(b->boxes.back().get());
+            }
+        } catch (...) {
+            cudaStreamSynchronize(0);  // no queued copy reads the caller's arrays after the call
+            throw;
         }
+        check_cuda(cudaStreamSynchronize(0), "upload");  // the caller's x, v are read by now
         b->batch.reset(new Batch(raw, cfg));
         // staging for state downloads, sized once for the largest box
         int nmax = 0;

@@ -221,13 +221,13 @@ Box::Box(const Spec &s, const Particles &p, int sms) : spec(s)
 }
 
 Box::Box(const Spec &s, int n_, const double *x, const double *v, const int32_t *tag, const int32_t *type,
-         const int32_t *mask, int sms)
+         const int32_t *mask, int sms, bool wait)
     : spec(s)
 {
     (void)sms;
     n = n_;
     try {
-        init(s, x, v, tag, type, mask);
+        init(s, x, v, tag, type, mask, wait);
     } catch (...) {
         release();
         throw;
@@ -235,7 +235,7 @@ Box::Box(const Spec &s, int n_, const double *x, const double *v, const int32_t 
 }
 
 void Box::init(const Spec &s, const double *x, const double *v, const int32_t *tag, const int32_t *type,
-               const int32_t *mask)
+               const int32_t *mask, bool wait)
 {
     if (n <= 0) throw std::runtime_error("ARG: box has no particles");
     if (s.ntype < 1 || s.ntype > kMaxTypes) throw std::runtime_error("ARG: 1..8 atom types supported");
@@ -358,7 +358,8 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     // Morton rank of every bin: reorder buckets are visited in Morton order of their bin
     {
         const std::vector<int> &rank = morton_ranks(g.mbin);
-        check_cuda(cudaMemcpy(B.bin_rank, rank.data(), sizeof(int) * nbin, cudaMemcpyHostToDevice), "upload");
+        // the cached ranks outlive the queued copy
+        check_cuda(cudaMemcpyAsync(B.bin_rank, rank.data(), sizeof(int) * nbin, cudaMemcpyHostToDevice, 0), "upload");
     }
     // initial state into buffer 0: the caller's AoS x and v go to the list table's space (unused
     // until the first build, which writes every entry it later reads), a kernel splits them
@@ -368,15 +369,15 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
         const size_t need = 6 * sizeof(double) * (size_t)n;
         if ((size_t)B.nrow * B.n_col * sizeof(int) < need) throw std::runtime_error("ARG: list table too small to stage");
         double *sx = reinterpret_cast<double *>(B.table), *sv = sx + 3 * (size_t)n;
-        check_cuda(cudaMemcpy(sx, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice), "upload");
-        if (v) check_cuda(cudaMemcpy(sv, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice), "upload");
-        if (tag) check_cuda(cudaMemcpy(B.tag[0], tag, sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
-        if (type) check_cuda(cudaMemcpy(B.type[0], type, sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
-        if (mask) check_cuda(cudaMemcpy(B.mask[0], mask, sizeof(int) * n, cudaMemcpyHostToDevice), "upload");
+        check_cuda(cudaMemcpyAsync(sx, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, 0), "upload");
+        if (v) check_cuda(cudaMemcpyAsync(sv, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, 0), "upload");
+        if (tag) check_cuda(cudaMemcpyAsync(B.tag[0], tag, sizeof(int) * n, cudaMemcpyHostToDevice, 0), "upload");
+        if (type) check_cuda(cudaMemcpyAsync(B.type[0], type, sizeof(int) * n, cudaMemcpyHostToDevice, 0), "upload");
+        if (mask) check_cuda(cudaMemcpyAsync(B.mask[0], mask, sizeof(int) * n, cudaMemcpyHostToDevice, 0), "upload");
         launch_load_state(0, sx, v ? sv : nullptr, n, B.x[0], B.xh, B.v[0], tag ? nullptr : B.tag[0],
                           type ? nullptr : B.type[0], mask ? nullptr : B.mask[0]);
         check_cuda(cudaGetLastError(), "upload");
-        check_cuda(cudaStreamSynchronize(0), "upload");
+        if (wait) check_cuda(cudaStreamSynchronize(0), "upload");
         if (mask) {
             for (int i = 0; i < n; ++i)
                 if (mask[i] & s.nve_bit) ++n_group;

@@ -64,9 +64,11 @@ class Box {
 public:
     Box(const Spec &spec, const Particles &p, int sms);
     // from caller arrays (AoS x[3n], v[3n]; v null: at rest; tag/type/mask null: tags 1..n,
-    // type 1, mask 1), copied straight to the device without host staging
+    // type 1, mask 1), copied straight to the device without host staging. wait = false leaves
+    // the copies queued on the legacy default stream: the caller synchronises it before it
+    // lets go of the arrays (a batch of boxes waits once, not once per box)
     Box(const Spec &spec, int n, const double *x, const double *v, const int32_t *tag, const int32_t *type,
-        const int32_t *mask, int sms);
+        const int32_t *mask, int sms, bool wait = true);
     ~Box();
     Box(const Box &) = delete;
     Box &operator=(const Box &) = delete;
@@ -99,7 +101,7 @@ private:
     void layout(const Spec &s, int na);
     void release() noexcept;  // returns the arena to the pool
     void init(const Spec &s, const double *x, const double *v, const int32_t *tag, const int32_t *type,
-              const int32_t *mask);
+              const int32_t *mask, bool wait = true);
     template <class T> T *alloc(size_t count);
 };
 
