@@ -41,7 +41,6 @@ __global__ void __launch_bounds__(128, density_blocks<kGather>()) k_density_rows
 {
     const int u = blockIdx.x;
     if (u >= nunits) return;
-    const int lane = threadIdx.x & 31;
     const Unit U = units[u];
     const BoxDesc &B = boxes[U.box];
     const int i = U.begin + threadIdx.x;

@@ -139,7 +139,9 @@ constexpr int kPartialStride = 18;  // see k_thermo_units for the slot map
 __host__ __device__ __forceinline__ void tea_core(uint32_t &v0, uint32_t &v1, int rounds)
 {
     uint32_t sum = 0;
+#ifdef __CUDA_ARCH__
 #pragma unroll
+#endif
     for (int r = 0; r < rounds; ++r) {
         sum += 0x9E3779B9u;
         v0 += ((v1 << 4) + 0xA341316Cu) ^ (v1 + sum) ^ ((v1 >> 5) + 0xC8013EA4u);
