@@ -503,7 +503,8 @@ __device__ __forceinline__ void list_put(int *table, int ncol, int cic, int base
     }
 }
 
-__global__ void __launch_bounds__(256, 5) k_rb_list(const BoxDesc *__restrict__ boxes,
+// 4 blocks per SM: 64 registers and no spill, measured faster than 5 blocks at 48 with a spill
+__global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ boxes,
                                                  const Unit *__restrict__ units, int nunits,
                                                  int nbox, int *done)
 {
@@ -655,7 +656,7 @@ void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const S
     scan<kSelBin>(s, boxes, u.scan_bin, u.nbox, sms);
     k_rb_scatter_bins<<<g(u.all.n, 8), kUnit, 0, s>>>(boxes, u.all.d, u.all.n);
     k_rb_bucket<1><<<g(u.bins.n, 5), 256, 0, s>>>(boxes, u.bins.d, u.bins.n);
-    k_rb_list<<<g(u.bins.n * 32, 5), 256, 0, s>>>(boxes, u.bins.d, u.bins.n, u.nbox, done + 1);
+    k_rb_list<<<g(u.bins.n * 32, 4), 256, 0, s>>>(boxes, u.bins.d, u.bins.n, u.nbox, done + 1);
 }
 
 }  // namespace mdpd
