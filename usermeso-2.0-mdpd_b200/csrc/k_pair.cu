@@ -1,8 +1,8 @@
 // mDPD pair passes with each pair evaluated once.
 //
 // k_density_rows: one lane per particle row of the full list (32 consecutive particles per
-//   warp, the locally transposed table makes each entry index a coalesced warp load), eight
-//   neighbour positions in flight per lane. It computes rho_i (fix_aboundary_rho_meso.cu:
+//   warp, the locally transposed table makes each entry index a coalesced warp load), G = 4, 6
+//   or 8 neighbour positions in flight per lane (the batch's autotuner picks G). It computes rho_i (fix_aboundary_rho_meso.cu:
 //   119-165) and writes, into the particle's row of the compact table, the entries within the
 //   force cutoff that the row owns: a local j when j > i, a ghost j when j is an image shifted
 //   in the positive direction (kUpperImage in pos.w). The mirrored pair, seen from the other
@@ -118,9 +118,9 @@ __device__ __forceinline__ void sadd64(unsigned *lo, unsigned *hi, long long q)
     atomicAdd(hi, qh + (old + ql < old ? 1u : 0u));
 }
 
-// 8 blocks per SM (64 registers) measured fastest against 6 and 7
+// 7 blocks per SM (up to 72 registers, no spill) measured fastest against 6 and 8
 template <bool EXACT, bool EV, bool UNI>
-__global__ void __launch_bounds__(128, 8) k_force_pairs(const BoxDesc *__restrict__ boxes,
+__global__ void __launch_bounds__(128, 7) k_force_pairs(const BoxDesc *__restrict__ boxes,
                                                         const Unit *__restrict__ units, int nunits)
 {
     __shared__ PairCoeff s_coeff[kMaxTypes * kMaxTypes];
