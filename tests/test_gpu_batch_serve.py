@@ -116,3 +116,14 @@ def test_autotuner_picks_a_shape_and_keeps_the_physics():
     d.step(20)
     assert d.thermo(0).status == 0
     d.close()
+
+
+def test_box_beyond_the_table_limit_is_refused():
+    # the list kernels address a box's neighbour table with unsigned 32-bit offsets: a box whose
+    # table would pass 2^32 entries (here through a density estimate that makes the rows long)
+    # is refused before anything is allocated, never silently wrapped
+    L = (100000 / 6.05) ** (1 / 3)
+    with pytest.raises(mdpd.MdpdError) as e:
+        mdpd.Batch([mdpd.box_spec(100000, L, rho_est=2.0e5, seed=3, init_seed=4)])
+    assert e.value.code == mdpd.ERR_ARG and "neighbour-table entries" in str(e.value)
+

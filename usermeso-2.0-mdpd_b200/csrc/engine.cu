@@ -336,11 +336,11 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     if (s.style == 0 && (long long)na >= (1LL << 27))
         throw std::runtime_error("ARG: box too large for one device box: " + std::to_string(na) +
                                  " particles and ghost images (limit 134217727)");
-    // the list kernels address the table with 32-bit offsets
-    if ((long long)B.nrow * B.n_col > 0x7fffffffLL)
+    // the list kernels address the table with unsigned 32-bit offsets
+    if ((long long)B.nrow * B.n_col > 0xffffffffLL)
         throw std::runtime_error("ARG: box too large for one device box: " + std::to_string(n) + " particles need " +
                                  std::to_string((long long)B.nrow * B.n_col) +
-                                 " neighbour-table entries (limit 2147483647); split it into boxes");
+                                 " neighbour-table entries (limit 4294967295); split it into boxes");
     layout(s, na);  // size the arena
     {
         void *a = nullptr;

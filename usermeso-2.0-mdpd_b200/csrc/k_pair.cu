@@ -53,7 +53,8 @@ __global__ void __launch_bounds__(128, density_blocks<kGather>()) k_density_rows
     const float4 pi = live ? B.pos[i] : make_float4(0, 0, 0, 0);
     const float h = B.cut_rho, h2 = h * h, rcf2 = B.rc2_force;
     const int ncol = B.n_col, nlocal = B.nlocal;
-    const int *row = B.table + (i & ~31) * ncol + (i & 31);  // entry k at (k & 31) * ncol + (k & ~31)
+    // unsigned 32-bit offsets: tables of up to 2^32 entries
+    const int *row = B.table + ((unsigned)(i & ~31) * (unsigned)ncol + (unsigned)(i & 31));  // entry k at (k & 31) * ncol + (k & ~31)
     const int ncol2 = B.n_col2;
     int *row2 = B.table2 + (size_t)i * ncol2;
     float acc = 0.f;

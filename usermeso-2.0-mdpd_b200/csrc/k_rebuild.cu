@@ -499,7 +499,7 @@ __device__ __forceinline__ void list_put(int *table, int ncol, int cic, int base
     if (hit) {
         const int p = base + __popc(bal & lt);
         if (p < ncol)
-            table[(cic & ~31) * ncol + (cic & 31) + (p & 31) * ncol + (p & ~31)] = j;
+            table[(unsigned)(cic & ~31) * (unsigned)ncol + (unsigned)((cic & 31) + (p & 31) * ncol + (p & ~31))] = j;
     }
 }
 

@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(kUnit *TPP, 16 / TPP) k_density(const BoxDesc 
             const float h = B.cut_rho, h2 = h * h;
             const int n = B.count[i];
             const int ncol = B.n_col;
-            const int *row = B.table + (i & ~31) * ncol + (i & 31);
+            const int *row = B.table + ((unsigned)(i & ~31) * (unsigned)ncol + (unsigned)(i & 31));
             // four independent index -> position gather chains in flight per thread
             for (int k0 = t; k0 < n; k0 += 4 * TPP) {
                 int j[4];
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(kUnit *TPP, 8 / TPP) k_force(const BoxDesc *__
             const float dtis = B.dt_inv_sqrt;
             const int n = B.count[i];
             const int ncol = B.n_col;
-            const int *row = B.table + (i & ~31) * ncol + (i & 31);
+            const int *row = B.table + ((unsigned)(i & ~31) * (unsigned)ncol + (unsigned)(i & 31));
             for (int kb = t; kb < n; kb += kQueue * TPP) {
                 // phase 1: distance test of up to kQueue entries, four gathers in flight;
                 // in-range neighbours are queued (this thread's column of s_q)

@@ -323,9 +323,9 @@ __device__ __forceinline__ float dist2(float dx, float dy, float dz)
 }
 
 // entry k of particle i in the locally transposed table
-__device__ __forceinline__ int list_addr(int i, int k, int n_col)
+__device__ __forceinline__ unsigned list_addr(int i, int k, int n_col)
 {
-    return ((i & ~31) + (k & 31)) * n_col + (k & ~31) + (i & 31);
+    return (unsigned)((i & ~31) + (k & 31)) * (unsigned)n_col + (unsigned)((k & ~31) + (i & 31));
 }
 
 __device__ __forceinline__ int clamp_bin(int i, int nmax)
