@@ -11,10 +11,13 @@
 //   ghosts   periodic images x + s*prd of every particle within cutghost of a face
 //            (MesoComm::borders, comm_meso.cu:42-193), binned with gpu_assign_bin_id's rule
 //            (neighbor_meso.cu:390-425)
-//   bins     the same bucket sort over locals+ghosts by bin, index order inside a bin
-//   list     warp per bin: 27-bin stencil candidates against up to 32 centres at a time,
-//            ballot insertion (atomic-free) straight into the locally transposed table
-//            (gpu_build_neighbor_list, neigh_build_meso.cu:17-127; layout neigh_list_meso.cu:143-147)
+//   bins     locals+ghosts by bin, index order inside a bin: a local's place follows from its
+//            reorder-class run; ghost images take atomic slots and bins holding them are sorted
+//   list     warp per bin: 27-bin stencil candidates filtered against the box of up to 32
+//            centres, then tested against each centre; every hit is written from the test
+//            ballot (atomic-free) straight into the locally transposed table, reduced rows on
+//            pair-once boxes (gpu_build_neighbor_list, neigh_build_meso.cu:17-127; layout
+//            neigh_list_meso.cu:143-147)
 #include "kernels.h"
 
 namespace mdpd {
