@@ -121,6 +121,10 @@ typedef struct mdpd_box_spec {
     const double *x, *v;
     uint64_t init_seed;
     double fill_lo[3], fill_hi[3];  /* random fill region (fill_hi <= fill_lo: whole box) */
+    /* timestep the box starts at: 0 for a new run; a restart passes the step its state was
+     * checkpointed at, so the pair RNG's step count (seed_now, pair_mdpd_meso.cu:295-297)
+     * continues as after a LAMMPS restart file (atom_vec_mdpd_atomic_meso.cu:530-607) */
+    int64_t start_step;
 } mdpd_box_spec;
 
 int mdpd_batch_create(mdpd_batch_t **b, const mdpd_box_spec *specs, int32_t nbox, const mdpd_opts *opts);
@@ -160,7 +164,7 @@ typedef struct mdpd_job_spec {
 } mdpd_job_spec;
 
 typedef struct mdpd_job_result {
-    int32_t state;        /* 0 queued, 1 running, 2 done, 3 failed, 4 cancelled */
+    int32_t state;        /* 0 queued, 1 running, 2 done, 3 failed, 4 cancelled, 5 preempted */
     int32_t error;        /* MDPD_* code when failed */
     int64_t steps_done;
     double submit_s, start_s, end_s;   /* host clock, seconds since server start */
@@ -173,8 +177,20 @@ int mdpd_box_bytes(const mdpd_box_spec *spec, uint64_t *bytes);
 int mdpd_server_start(mdpd_server_t **s, uint64_t budget_bytes, const mdpd_opts *opts);
 int mdpd_server_submit(mdpd_server_t *s, const mdpd_job_spec *job, int64_t *job_id);
 int mdpd_server_poll(mdpd_server_t *s, int64_t job_id, mdpd_job_result *out);
+/* x, v (tag order, 3n each) of a done job kept with keep_state, or the checkpoint of a
+ * preempted one; MDPD_ERR_STATE when there is none */
 int mdpd_server_get_state(mdpd_server_t *s, int64_t job_id, double *x, double *v, int64_t n);
 int mdpd_server_cancel(mdpd_server_t *s, int64_t job_id);
+/* checkpoint and release a job (preemption, migration to another server or GPU): a running
+ * job stops at the end of its current chunk of steps, its x, v are kept on the host and it
+ * ends in state 5 with steps_done and thermo.step set; a queued one ends in state 5 at once,
+ * its checkpoint the x, v it was submitted with (if any). Resubmitting the box with those
+ * x, v, start_step = thermo.step and the remaining steps resumes it, as a run continued from
+ * a LAMMPS restart file would (pack/unpack_restart, atom_vec_mdpd_atomic_meso.cu:530-607):
+ * the same random-number steps, forces recomputed at setup from x and v (the integrator's
+ * dissipative force then sees v at the full step once, where the running job had the half
+ * step, so the continuation is statistically, not bitwise, the uninterrupted run) */
+int mdpd_server_preempt(mdpd_server_t *s, int64_t job_id);
 /* wait until every submitted job is done, failed or cancelled (timeout_s <= 0: no limit) */
 int mdpd_server_drain(mdpd_server_t *s, double timeout_s);
 /* throughput/latency summary: particle-steps/s, step p50/p99 ms, job p50/p99 s,

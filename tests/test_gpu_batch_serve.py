@@ -127,3 +127,48 @@ def test_box_beyond_the_table_limit_is_refused():
         mdpd.Batch([mdpd.box_spec(100000, L, rho_est=2.0e5, seed=3, init_seed=4)])
     assert e.value.code == mdpd.ERR_ARG and "neighbour-table entries" in str(e.value)
 
+
+def test_server_preempt_checkpoint_and_resume():
+    # a preempted job leaves its x, v and step as a checkpoint, equal bit for bit to the
+    # uninterrupted run at that step; the box resubmitted from it (start_step) continues the run
+    # with the same random-number steps. As after a LAMMPS restart (x and v stored, forces
+    # recomputed at setup), its first forces see v at the full step where the running integrator
+    # had the half step, so 10 steps on it is close to the uninterrupted job but not equal; a
+    # resume at the wrong step draws other random forces and is far further off.
+    n = 20000
+    L = (n / 6.05) ** (1 / 3)
+
+    def spec(**kw):
+        return mdpd.box_spec(n, L, A=-40.0, B=25.0, seed=77, init_seed=5, **kw)
+
+    srv = mdpd.Server(20 << 30)
+    b = srv.submit(spec(), 4000, keep_state=True)
+    t0 = time.time()
+    while srv.poll(b).steps_done == 0 and time.time() - t0 < 60:
+        time.sleep(0.001)
+    srv.preempt(b)
+    srv.drain(120)
+    rb = srv.poll(b)
+    d = rb.steps_done
+    assert rb.state == 5 and 0 < d < 4000 and rb.thermo.step == d
+    xb, vb = srv.state(b, n)
+    with pytest.raises(mdpd.MdpdError):
+        srv.preempt(b)  # already ended
+    c = srv.submit(spec(), d, keep_state=True)
+    e = srv.submit(spec(), d + 10, keep_state=True)
+    r = srv.submit(spec(x=xb, v=vb, start_step=d), 10, keep_state=True)
+    w = srv.submit(spec(x=xb, v=vb), 10, keep_state=True)  # restarted at step 0: wrong RNG steps
+    srv.drain(120)
+    xc, vc = srv.state(c, n)
+    assert np.array_equal(xc, xb) and np.array_equal(vc, vb)  # the checkpoint is the run at step d
+    assert srv.poll(r).thermo.step == d + 10
+    xe, ve = srv.state(e, n)
+    xr, vr = srv.state(r, n)
+    _, vw = srv.state(w, n)
+    srv.stop()
+    dv_r = np.sqrt(np.mean((vr - ve) ** 2))
+    dv_w = np.sqrt(np.mean((vw - ve) ** 2))
+    assert dv_r < 0.1 * dv_w and dv_w > 0.1, (dv_r, dv_w)
+    dx = np.mod(xr - xe + L / 2, L) - L / 2
+    assert np.abs(dx).max() < 1e-2
+

@@ -374,6 +374,8 @@ void spec_from_box(const mdpd_box_spec &bs, Spec &s, Particles &p)
     s.mass[0] = bs.mass > 0 ? bs.mass : 1.0;
     s.cut_rho = bs.cut_rho > 0 ? bs.cut_rho : 0.75;
     s.exact_rng = bs.exact_rng;
+    if (bs.start_step < 0) throw std::runtime_error("ARG: box spec with start_step < 0");
+    s.step0 = bs.start_step;
     PairParam q;
     q.set = 1;
     q.A = bs.A, q.B = bs.B, q.gamma = bs.gamma, q.cut = bs.cut > 0 ? bs.cut : 1.0;

@@ -353,6 +353,11 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     }
     check_cuda(cudaMemsetAsync(arena_, 0, arena_need_, 0), "memset");
     layout(s, na);  // hand out the pieces
+    if (s.step0 != 0) {  // a restarted box: its step counter continues (after the memset, same stream)
+        BoxState st{};
+        st.step = s.step0;
+        check_cuda(cudaMemcpy(d_state, &st, sizeof(st), cudaMemcpyHostToDevice), "state");
+    }
     bytes = arena_need_;
 
     // Morton rank of every bin: reorder buckets are visited in Morton order of their bin

@@ -41,6 +41,7 @@ struct Spec {
     double ab_rho0 = 0, ab_sigma = 0;
     int exact_rng = 0;
     double ghost_factor = 1.0;   // ghost capacity multiplier
+    long long step0 = 0;         // timestep the box starts at (a restart continues the RNG's steps)
 };
 
 struct Particles {

@@ -1,7 +1,9 @@
 // Serving loop: jobs (boxes + step counts) are admitted while their device footprint fits
 // the HBM budget, stay resident until done, and are stepped together by the batched graph.
 // Arrivals and retirements change the batch between chunks of steps (continuous batching).
-// One driver thread issues all device work; submit/poll/cancel only touch the queue.
+// One driver thread issues all device work; submit/poll/cancel/preempt only touch the queue.
+// A preempted job leaves with its x, v (tag order) and step count kept on the host: its
+// checkpoint, from which a resubmitted box (start_step) continues the run.
 //
 // The reference's only form of many simulations is one LAMMPS instance per MPI rank
 // group (main_ensemble, src/main.cpp:49-117); here they share one GPU and one launch.
@@ -41,6 +43,7 @@ struct Job {
     std::unique_ptr<Box> box;
     size_t bytes = 0;
     bool cancel = false;
+    bool preempt = false;
 };
 
 double pct(std::vector<float> v, double p)
@@ -100,6 +103,15 @@ void mdpd_server_s::loop()
                 std::shared_ptr<Job> j = jobs[queue.front()];
                 if (j->cancel) {
                     j->state = 4;
+                    queue.pop_front();
+                    continue;
+                }
+                if (j->preempt) {  // never started: its checkpoint is what it was submitted with
+                    j->state = 5;
+                    j->thermo.step = j->spec.box.start_step;
+                    j->xf = j->x0;
+                    j->vf = j->v0.empty() && !j->x0.empty() ? std::vector<double>(j->x0.size(), 0.0) : j->v0;
+                    j->end_s = now();
                     queue.pop_front();
                     continue;
                 }
@@ -195,7 +207,9 @@ void mdpd_server_s::loop()
             j->done += k;
             for (int64_t s = 0; s < k; ++s) j->step_ms.push_back(ms / k);
             const bool fail = bst.status != 0;
-            if (j->done >= j->spec.nsteps || fail || j->cancel) {
+            const bool finished = j->done >= j->spec.nsteps;
+            const bool preempted = j->preempt && !finished && !fail && !j->cancel;
+            if (finished || fail || j->cancel || preempted) {
                 if (th.empty()) batch->thermo(th);
                 Thermo t = th[q];
                 mdpd_thermo_t out{};
@@ -211,7 +225,7 @@ void mdpd_server_s::loop()
                 out.surface_tension = t.surface_tension;
                 out.status = t.status;
                 std::vector<double> xf, vf;
-                if (j->spec.keep_state && !fail) {
+                if ((j->spec.keep_state || preempted) && !fail) {
                     const int n = j->box->n;
                     xf.resize(3 * (size_t)n);
                     vf.resize(3 * (size_t)n);
@@ -221,10 +235,10 @@ void mdpd_server_s::loop()
                 j->thermo = out;
                 j->xf.swap(xf);
                 j->vf.swap(vf);
-                j->state = fail ? 3 : j->cancel ? 4 : 2;
+                j->state = fail ? 3 : j->cancel ? 4 : preempted ? 5 : 2;
                 if (fail) j->error = (bst.status & kErrNonFinite) ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW;
                 j->end_s = now();
-                job_latency_s.push_back(j->end_s - j->submit_s);
+                if (!preempted) job_latency_s.push_back(j->end_s - j->submit_s);  // a preempted job goes on elsewhere
                 resident -= j->bytes;
                 retired = true;
             } else
@@ -334,7 +348,7 @@ int mdpd_server_get_state(mdpd_server_t *s, int64_t id, double *x, double *v, in
     auto it = s->jobs.find(id);
     if (it == s->jobs.end()) return MDPD_ERR_ARG;
     const Job &j = *it->second;
-    if (j.state != 2 || j.xf.empty()) return MDPD_ERR_STATE;
+    if ((j.state != 2 && j.state != 5) || j.xf.empty()) return MDPD_ERR_STATE;
     if ((int64_t)j.xf.size() != 3 * n) return MDPD_ERR_ARG;
     if (x) std::copy(j.xf.begin(), j.xf.end(), x);
     if (v) std::copy(j.vf.begin(), j.vf.end(), v);
@@ -348,6 +362,18 @@ int mdpd_server_cancel(mdpd_server_t *s, int64_t id)
     auto it = s->jobs.find(id);
     if (it == s->jobs.end()) return MDPD_ERR_ARG;
     it->second->cancel = true;
+    s->cv.notify_all();
+    return MDPD_OK;
+}
+
+int mdpd_server_preempt(mdpd_server_t *s, int64_t id)
+{
+    if (!s) return MDPD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(id);
+    if (it == s->jobs.end()) return MDPD_ERR_ARG;
+    if (it->second->state >= 2) return MDPD_ERR_STATE;  // already ended
+    it->second->preempt = true;
     s->cv.notify_all();
     return MDPD_OK;
 }

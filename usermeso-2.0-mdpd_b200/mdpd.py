@@ -43,7 +43,7 @@ class BoxSpec(C.Structure):
                 ("seed", C.c_uint32), ("every", C.c_int32), ("delay", C.c_int32), ("check", C.c_int32),
                 ("exact_rng", C.c_int32),
                 ("x", C.POINTER(C.c_double)), ("v", C.POINTER(C.c_double)), ("init_seed", C.c_uint64),
-                ("fill_lo", C.c_double * 3), ("fill_hi", C.c_double * 3)]
+                ("fill_lo", C.c_double * 3), ("fill_hi", C.c_double * 3), ("start_step", C.c_int64)]
 
 
 class JobSpec(C.Structure):
@@ -239,7 +239,7 @@ def gaussian(si, sj, exact=True, fast=True):
 
 def box_spec(n, L, style=0, A=-40.0, B=25.0, gamma=4.5, kT=1.0, cut=1.0, cut_r=0.75, cut_rho=0.75,
              sigma=3.0, dt=0.01, skin=0.3, rho_est=6.05, mass=1.0, seed=1234, every=1, delay=0, check=1,
-             exact_rng=0, x=None, v=None, init_seed=1, fill_lo=(0, 0, 0), fill_hi=(0, 0, 0), lo=None):
+             exact_rng=0, x=None, v=None, init_seed=1, fill_lo=(0, 0, 0), fill_hi=(0, 0, 0), lo=None, start_step=0):
     L = np.broadcast_to(np.asarray(L, float), (3,))
     lo = np.zeros(3) if lo is None else np.asarray(lo, float)
     s = BoxSpec()
@@ -255,6 +255,7 @@ def box_spec(n, L, style=0, A=-40.0, B=25.0, gamma=4.5, kT=1.0, cut=1.0, cut_r=0
         v = np.ascontiguousarray(v, np.float64); s._keep.append(v); s.v = _ptr(v, C.c_double)
     s.init_seed = init_seed
     s.fill_lo[:] = list(fill_lo); s.fill_hi[:] = list(fill_hi)
+    s.start_step = int(start_step)
     return s
 
 
@@ -380,6 +381,13 @@ class Server:
 
     def cancel(self, jid):
         lib().mdpd_server_cancel(self.h, jid)
+
+    def preempt(self, jid):
+        """checkpoint and release a job (state 5): state(jid, n) then returns its x, v and
+        poll(jid).thermo.step the step to resubmit it from (box_spec(..., start_step=...))"""
+        rc = lib().mdpd_server_preempt(self.h, jid)
+        if rc:
+            raise MdpdError(rc, "preempt refused")
 
     def drain(self, timeout_s=0.0):
         rc = lib().mdpd_server_drain(self.h, float(timeout_s))
