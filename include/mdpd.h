@@ -54,7 +54,9 @@ typedef struct mdpd_thermo_t {
     double temp_group;    /* temperature of the nve/meso group */
     double ptensor[6];    /* pressure tensor (kinetic + virial)/V: xx yy zz xy xz yz */
     double surface_tension; /* (Lx/2)(Pxx - (Pyy+Pzz)/2) for a slab normal to x */
-    int32_t status;       /* device error bits */
+    int32_t status;       /* device error bits: 1 list, 2 ghost, 4 bin/bucket overflow, 8 non-finite
+                             force, 16 particle lost, 32 compact list overflow, 64 index out of
+                             range (index-check build) */
     int32_t pad;
 } mdpd_thermo_t;
 
@@ -101,6 +103,15 @@ int mdpd_get_pairs(mdpd_t *h, int32_t *tag_i, int32_t *tag_j, int64_t cap, int64
 
 /* --- pairwise RNG on explicit signature pairs (math_meso.h:465-473) --------------------- */
 int mdpd_gaussian(const uint32_t *si, const uint32_t *sj, double *exact, float *fast, int64_t n);
+
+/* --- build variant ------------------------------------------------------------------------ */
+/* 1 when this library is the index-check build (libmdpd_check.so: `build.py --check`, compiled
+ * with -DMDPD_CHECK), 0 for libmdpd.so.  The check build bounds-checks every neighbour, bin,
+ * bucket and permutation index its kernels use; an index outside its array sets bit 64 of the
+ * box's status word (mdpd_thermo_t.status), the access is skipped, and the run returns
+ * MDPD_ERR_OVERFLOW naming the bit.  No reference counterpart: the reference only syncs and
+ * gathers CUDA errors in its debug build (mvv_meso.cu:41-73). */
+int mdpd_index_checks(void);
 
 /* --- batched boxes: many independent boxes stepped by one graph per step ---------------- */
 typedef struct mdpd_batch_s mdpd_batch_t;

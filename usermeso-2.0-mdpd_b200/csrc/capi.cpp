@@ -324,6 +324,15 @@ int mdpd_get_pairs(mdpd_t *h, int32_t *ti, int32_t *tj, int64_t cap, int64_t *np
     });
 }
 
+int mdpd_index_checks(void)
+{
+#ifdef MDPD_CHECK
+    return 1;
+#else
+    return 0;
+#endif
+}
+
 int mdpd_gaussian(const uint32_t *si, const uint32_t *sj, double *exact, float *fast, int64_t n)
 {
     if (!si || !sj || n < 0) return MDPD_ERR_ARG;

@@ -738,6 +738,18 @@ void Batch::read_states(std::vector<BoxState> &out)
     check_cuda(cudaStreamSynchronize(stream_), "states");
 }
 
+// names of the set bits of a box status word
+std::string status_text(int bits)
+{
+    static const char *names[] = {"neighbour list overflow", "ghost capacity overflow", "bin/bucket overflow",
+                                  "non-finite force", "particle lost", "compact list overflow",
+                                  "index out of range (index-check build)"};
+    std::string t;
+    for (int k = 0; k < 7; ++k)
+        if (bits & (1 << k)) t += (t.empty() ? "" : ", ") + std::string(names[k]);
+    return t;
+}
+
 int Batch::status(std::string &msg)
 {
     int all = 0;
@@ -747,7 +759,8 @@ int Batch::status(std::string &msg)
         const BoxState &st = sts[b];
         if (st.status) {
             all |= st.status;
-            msg += "box " + std::to_string(b) + ": status " + std::to_string(st.status) + "; ";
+            msg += "box " + std::to_string(b) + ": status " + std::to_string(st.status) + " (" +
+                   status_text(st.status) + "); ";
         }
     }
     return all;

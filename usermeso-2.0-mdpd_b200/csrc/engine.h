@@ -147,6 +147,7 @@ private:
     void capture(int ev);
 };
 
+std::string status_text(int bits);  // names of the set bits of a box status word
 std::string cuda_err(cudaError_t e);
 void check_cuda(cudaError_t e, const char *what);
 int sm_count();

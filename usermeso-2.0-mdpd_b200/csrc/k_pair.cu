@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(128, density_blocks<kGather>()) k_density_rows
     const bool live = i < U.end;
     const int c = B.st->cur;
     const bool in_group = live && (B.mask[c][i] & B.rho_bit);
-    const int n = live ? B.count[i] : 0;
+    const int n = live ? MDPD_IDX(B.count[i], B.n_col + 1) : 0;
     int nmax = n;
     for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
     const float4 pi = live ? B.pos[i] : make_float4(0, 0, 0, 0);
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(128, density_blocks<kGather>()) k_density_rows
 #pragma unroll
         for (int q = 0; q < kGather; ++q) {
             const int k = k0 + q;
-            j[q] = k < n ? __ldcs(row + (k & 31) * ncol + (k & ~31)) : -1;
+            j[q] = k < n ? MDPD_IDX(__ldcs(row + (k & 31) * ncol + (k & ~31)), n_all(B)) : -1;
         }
 #pragma unroll
         for (int q = 0; q < kGather; ++q) pj[q] = j[q] >= 0 ? __ldg(&B.pos[j[q]]) : make_float4(1e30f, 0, 0, 0);
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(128, 7) k_force_pairs(const BoxDesc *__restric
         s_pi[t] = B.pos[i];
         s_vi[t] = B.vel[i];
         s_rho[t] = B.rho[i];
-        pre = B.count2[i];
+        pre = MDPD_IDX(B.count2[i], B.n_col2 + 1);
     }
     for (int o = 1; o < 32; o <<= 1) {
         const int v = __shfl_up_sync(0xffffffffu, pre, o);
@@ -172,9 +172,9 @@ __global__ void __launch_bounds__(128, 7) k_force_pairs(const BoxDesc *__restric
         long long ax = 0, ay = 0, az = 0;
         // j's state for the next entry is loaded while the current pair is evaluated
         const int en = __ldcs(B.table2 + (size_t)(i0 + r) * ncol2 + (m0 - rbeg));
-        int jn = en & kEntryIndex, tn = en >> kEntryTypeShift;
+        int jn = MDPD_IDX(en & kEntryIndex, n_all(B)), tn = en >> kEntryTypeShift;
         float4 pjn = __ldg(&B.posrho[jn]), vjn = __ldg(&B.vel[jn]);
-        int srcn = jn < nlocal ? jn : __ldg(&B.gsrc[jn - nlocal]);
+        int srcn = jn < nlocal ? jn : MDPD_IDX(__ldg(&B.gsrc[jn - nlocal]), nlocal);
         for (int m = m0; m < m1; ++m) {
             if (m >= rend) {  // the share moves on to the next non-empty row
                 sadd64(&s_lo[0][wb + r], &s_hi[0][wb + r], ax);
@@ -199,11 +199,11 @@ __global__ void __launch_bounds__(128, 7) k_force_pairs(const BoxDesc *__restric
                     re = P[rr + 1];
                 }
                 const int e = __ldcs(B.table2 + (size_t)(i0 + rr) * ncol2 + (m + 1 - rb));
-                const int jj = e & kEntryIndex;
+                const int jj = MDPD_IDX(e & kEntryIndex, n_all(B));
                 tn = e >> kEntryTypeShift;
                 pjn = __ldg(&B.posrho[jj]);
                 vjn = __ldg(&B.vel[jj]);
-                srcn = jj < nlocal ? jj : __ldg(&B.gsrc[jj - nlocal]);
+                srcn = jj < nlocal ? jj : MDPD_IDX(__ldg(&B.gsrc[jj - nlocal]), nlocal);
             }
             const PairCoeff &cf = s_coeff[UNI ? 0 : ptype(pi) * ntype + tj];
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;

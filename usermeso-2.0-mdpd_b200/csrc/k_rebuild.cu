@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(kUnit) k_rb_key(const BoxDesc *__restrict__ bo
             border |= (x <= B.lo[d] + B.cutghost) || (x >= B.hi[d] - B.cutghost);
         }
         const int bin = (int)(bid[0] + B.mbin[0] * (bid[1] + bid[2] * B.mbin[1]));
-        const int cls = (border ? B.nbin : 0) + B.bin_rank[bin];
+        const int cls = MDPD_IDX((border ? B.nbin : 0) + B.bin_rank[MDPD_IDX(bin, B.nbin)], 2 * B.nbin);
         B.cls_of[i] = cls;
         B.sub_of[i] = (int)morton3(sub[0], sub[1], sub[2]);
         atomicAdd(&B.cls_count[cls], 1);
@@ -218,8 +218,8 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_cls(const BoxDesc *__restr
         if (!rebuilding(B)) continue;
         const int i = U.begin + threadIdx.x;
         if (i >= U.end) continue;
-        const int p = atomicAdd(&B.cls_cursor[B.cls_of[i]], 1);
-        B.perm[p] = i;
+        const int p = atomicAdd(&B.cls_cursor[MDPD_IDX(B.cls_of[i], 2 * B.nbin)], 1);
+        B.perm[MDPD_IDX(p, B.nlocal)] = i;
     }
 }
 
@@ -245,6 +245,10 @@ __global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict_
             if (n == 0) continue;
             const int s = start[b];
             __syncwarp();
+            if (!(MDPD_IN(s, s + n) && MDPD_IN(s + n - 1, MODE == 0 ? B.nlocal : n_all(B)))) {
+                if (lane == 0) cnt[b] = 0;  // check build: a bucket outside its array
+                continue;
+            }
             if (MODE == 1 && arr[s + n - 1] < B.nlocal) {
                 // locals only: already in index order, bpos written by the scatter
                 if (lane == 0) cnt[b] = 0;
@@ -258,7 +262,7 @@ __global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict_
                 continue;
             }
             for (int e = lane; e < n; e += 32) {
-                const int idx = arr[s + e];
+                const int idx = MDPD_IDX(arr[s + e], MODE == 0 ? B.nlocal : n_all(B));
                 key[e] = MODE == 0 ? (((unsigned long long)(uint32_t)B.sub_of[idx] << 32) | (uint32_t)idx)
                                    : (unsigned long long)(uint32_t)idx;
             }
@@ -304,7 +308,7 @@ __global__ void __launch_bounds__(kUnit) k_rb_permute(BoxDesc *__restrict__ boxe
         if (k >= U.end) continue;
         const BoxState &S = *B.st;
         const int c = S.cur, o = 1 - c;
-        const int old = B.perm[k];
+        const int old = MDPD_IDX(B.perm[k], B.nlocal);
         // every load of the particle is issued before the first store (the compiler may not move
         // a load above a store to a possibly aliased array): one memory round trip
         double x[3], v[3];
@@ -345,7 +349,7 @@ __global__ void __launch_bounds__(kUnit) k_rb_permute(BoxDesc *__restrict__ boxe
         for (int d = 0; d < 3; ++d) bid[d] = clamp_bin(bin_coord(x[d], B.lo[d], B.bininv[d]), B.mbin[d]);
         const int bin = bid[0] + B.mbin[0] * (bid[1] + bid[2] * B.mbin[1]);
         B.bin_of[k] = bin;
-        atomicAdd(&B.bin_count[bin], 1);
+        atomicAdd(&B.bin_count[MDPD_IDX(bin, B.nbin)], 1);
     }
     __shared__ bool s_last;
     __syncthreads();
@@ -423,7 +427,7 @@ __global__ void __launch_bounds__(kUnit) k_rb_ghosts(const BoxDesc *__restrict__
                     }
                     const int bin = bid[0] + B.mbin[0] * (bid[1] + bid[2] * B.mbin[1]);
                     B.bin_of[gi] = bin;
-                    atomicAdd(&B.bin_count[bin], 1);
+                    atomicAdd(&B.bin_count[MDPD_IDX(bin, B.nbin)], 1);
                     ++g;
                 }
             }
@@ -448,17 +452,17 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__rest
         const int i = U.begin + threadIdx.x;
         const int nl = B.nlocal;
         if (i >= U.end || i >= nl + min(B.st->nghost, B.ghost_cap)) continue;
-        const int bin = B.bin_of[i];
+        const int bin = MDPD_IDX(B.bin_of[i], B.nbin);
         const int rk = B.bin_rank[bin];
         const int b0 = B.cls_start[rk], b1 = B.cls_start[rk + 1];  // the bin's bulk run
         const int e0 = B.cls_start[B.nbin + rk];                     // its border run
         int p;
         if (i < nl) {
-            p = B.bin_start[bin] + (i < B.st->n_bulk ? i - b0 : (b1 - b0) + (i - e0));
+            p = MDPD_IDX(B.bin_start[bin] + (i < B.st->n_bulk ? i - b0 : (b1 - b0) + (i - e0)), n_all(B));
             B.bpos[p] = B.pos[i];
         } else {
             const int nloc = (b1 - b0) + (B.cls_start[B.nbin + rk + 1] - e0);
-            p = atomicAdd(&B.bin_cursor[bin], 1) + nloc;
+            p = MDPD_IDX(atomicAdd(&B.bin_cursor[bin], 1) + nloc, n_all(B));
         }
         B.bin_order[p] = i;
     }
@@ -524,7 +528,9 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
         const int b = U.begin + ((it & 31) << 3) + w;
         if (b >= U.end) continue;
         const int s = B.bin_start[b], e = B.bin_start[b + 1];
-        if (e == s || B.bin_order[s] >= B.nlocal) continue;  // no locals in this bin
+        if (e == s) continue;
+        if (!(MDPD_IN(s, e) && MDPD_IN(e - 1, n_all(B)))) continue;  // check build: a bin outside the arrays
+        if (B.bin_order[s] >= B.nlocal) continue;  // no locals in this bin
         const float rc2 = B.rc2_tail;
         const float rn2 = B.list_reduce ? B.rn2_list : rc2;  // with rc2: every pair (full list)
         const int ncol = B.n_col, nlocal = B.nlocal;
@@ -538,6 +544,7 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
                 const int nb = x + B.mbin[0] * (y + z * B.mbin[1]);
                 st = B.bin_start[nb];
                 sz = B.bin_start[nb + 1] - st;
+                if (sz != 0 && !(MDPD_IN(st, st + sz) && MDPD_IN(st + sz - 1, n_all(B)))) sz = 0;
             }
         }
         int cum = sz;
@@ -554,7 +561,7 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
         for (int cb = s; cb < e; cb += 32) {
             // centre batch: members with index < nlocal (they come first in a bin)
             const int pc = cb + lane;
-            const int ci = pc < e ? B.bin_order[pc] : nlocal;
+            const int ci = pc < e ? MDPD_IDX(B.bin_order[pc], n_all(B)) : nlocal;
             const bool is_c = ci < nlocal;
             const unsigned cm = __ballot_sync(0xffffffffu, is_c);
             if (cm == 0) break;
@@ -581,7 +588,7 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
                         while (s_cum[w][slot + 1] <= q) ++slot;
                         const int p = s_bs[w][slot] + (q - s_cum[w][slot]);
                         pj = B.bpos[p];
-                        j = B.bin_order[p];
+                        j = MDPD_IDX(B.bin_order[p], n_all(B));
                         const float gx = fmaxf(fmaxf(lox - pj.x, pj.x - hix), 0.f);
                         const float gy = fmaxf(fmaxf(loy - pj.y, pj.y - hiy), 0.f);
                         const float gz = fmaxf(fmaxf(loz - pj.z, pj.z - hiz), 0.f);

@@ -96,15 +96,15 @@ __global__ void __launch_bounds__(kUnit, integrate_blocks(WALL)) k_integrate(Box
                 const float cx = (float)x, cy = (float)y, cz = (float)z;
                 double phi_i = 0.0;
                 float nx = 0.f, ny = 0.f, nz = 0.f;
-                const int n = B.count[i];
+                const int n = MDPD_IDX(B.count[i], B.n_col + 1);
                 const float cp = B.cut_phi;
                 for (int k = 0; k < n; ++k) {
-                    const int j = B.table[list_addr(i, k, B.n_col)];
+                    const int j = MDPD_IDX(B.table[list_addr(i, k, B.n_col)], n_all(B));
                     const float4 pj = B.pos[j];
                     if (!(pflags(pj) & 2)) continue;
                     int s = j, code = 13;
                     if (j >= B.nlocal) {
-                        s = B.gsrc[j - B.nlocal];
+                        s = MDPD_IDX(B.gsrc[j - B.nlocal], B.nlocal);
                         code = B.gimg[j - B.nlocal];
                     }
                     const float jx = (float)(B.x[c][0][s] + (code % 3 - 1) * B.prd[0]);
@@ -239,7 +239,7 @@ __device__ __forceinline__ float3 packed_at_build(const BoxDesc &B, int j)
 {
     int s = j, code = 13;
     if (j >= B.nlocal) {
-        s = B.gsrc[j - B.nlocal];
+        s = MDPD_IDX(B.gsrc[j - B.nlocal], B.nlocal);
         code = B.gimg[j - B.nlocal];
     }
     return make_float3((float)(B.xh[0][s] + (code % 3 - 1) * B.prd[0] - B.cen[0]),
@@ -282,10 +282,10 @@ __global__ void __launch_bounds__(kUnit) k_aboundary_meso(BoxDesc *__restrict__ 
         const float sig = B.ab_sigma, rc2 = B.rc2_core, nf = B.ab_nfactor;
         const float ex = __fdiv_rn(-0.5f, sig);
         float rho_w = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-        const int n = B.count[i];
+        const int n = MDPD_IDX(B.count[i], B.n_col + 1);
         for (int k = 0; k < n; ++k) {
-            const int j = B.table[list_addr(i, k, B.n_col)];
-            const int mj = j < B.nlocal ? B.mask[c][j] : B.mask[c][B.gsrc[j - B.nlocal]];
+            const int j = MDPD_IDX(B.table[list_addr(i, k, B.n_col)], n_all(B));
+            const int mj = j < B.nlocal ? B.mask[c][j] : B.mask[c][MDPD_IDX(B.gsrc[j - B.nlocal], B.nlocal)];
             if (!(mj & B.ab_wall_bit)) continue;
             const float3 bj = packed_at_build(B, j);
             if (!(dist2(bi.x - bj.x, bi.y - bj.y, bi.z - bj.z) <= rc2)) continue;  // not a core entry
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(kUnit *TPP, 16 / TPP) k_density(const BoxDesc 
         if (in_group) {
             const float4 pi = B.pos[i];
             const float h = B.cut_rho, h2 = h * h;
-            const int n = B.count[i];
+            const int n = MDPD_IDX(B.count[i], B.n_col + 1);
             const int ncol = B.n_col;
             const int *row = B.table + ((unsigned)(i & ~31) * (unsigned)ncol + (unsigned)(i & 31));
             // four independent index -> position gather chains in flight per thread
@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(kUnit *TPP, 16 / TPP) k_density(const BoxDesc 
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int k = k0 + q * TPP;
-                    j[q] = k < n ? __ldcs(row + (k & 31) * ncol + (k & ~31)) : -1;
+                    j[q] = k < n ? MDPD_IDX(__ldcs(row + (k & 31) * ncol + (k & ~31)), n_all(B)) : -1;
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q) pj[q] = j[q] >= 0 ? __ldg(&B.pos[j[q]]) : make_float4(1e30f, 0, 0, 0);
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(kUnit *TPP, 8 / TPP) k_force(const BoxDesc *__
                 wall_sqrt = sqrtf(wall_ratio);
             }
             const float dtis = B.dt_inv_sqrt;
-            const int n = B.count[i];
+            const int n = MDPD_IDX(B.count[i], B.n_col + 1);
             const int ncol = B.n_col;
             const int *row = B.table + ((unsigned)(i & ~31) * (unsigned)ncol + (unsigned)(i & 31));
             for (int kb = t; kb < n; kb += kQueue * TPP) {
@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(kUnit *TPP, 8 / TPP) k_force(const BoxDesc *__
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const int k = kb + (b4 + q) * TPP;
-                        j[q] = k < n ? __ldcs(row + (k & 31) * ncol + (k & ~31)) : -1;
+                        j[q] = k < n ? MDPD_IDX(__ldcs(row + (k & 31) * ncol + (k & ~31)), n_all(B)) : -1;
                     }
 #pragma unroll
                     for (int q = 0; q < 4; ++q)

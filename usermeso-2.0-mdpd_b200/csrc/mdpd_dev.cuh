@@ -23,6 +23,7 @@ enum : int {
     kErrNonFinite = 8,      // NaN/Inf force
     kErrLost = 16,          // particle outside the box by more than one period
     kErrList2Overflow = 32, // more force-range neighbours than the compact list holds
+    kErrIndex = 64,         // check build: an index outside its array (the access was skipped)
 };
 
 struct PairCoeff {  // per type pair; FP32 pair arithmetic
@@ -320,6 +321,44 @@ __device__ __forceinline__ float gaussian_fast(uint32_t si, uint32_t sj)
 __device__ __forceinline__ float dist2(float dx, float dy, float dz)
 {
     return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+}
+
+// ---------------------------------------------------------------------------
+// Index checks of the check build (compiled with -DMDPD_CHECK; `build.py --check` writes
+// libmdpd_check.so).  MDPD_IDX(i, n) is i when 0 <= i < n; otherwise it sets kErrIndex in the
+// status word of the box B in scope and gives 0, an index every array of the box holds, so the
+// access stays in bounds and the host reads the error after the step.  Nothing traps.  In the
+// normal build MDPD_IDX(i, n) is i and n is not evaluated.  MDPD_IN(i, n) is the same test as
+// a condition (always true in the normal build), for a range the caller skips as a whole.
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ bool index_ok(long long i, long long n, int *status)
+{
+    if (i >= 0 && i < n) return true;
+#ifdef __CUDA_ARCH__
+    atomicOr(status, kErrIndex);
+#else
+    __atomic_fetch_or(status, kErrIndex, __ATOMIC_RELAXED);
+#endif
+    return false;
+}
+
+__host__ __device__ __forceinline__ int checked_index(long long i, long long n, int *status)
+{
+    return index_ok(i, n, status) ? (int)i : 0;
+}
+
+#ifdef MDPD_CHECK
+#define MDPD_IDX(i, n) ::mdpd::checked_index((i), (n), &B.st->status)
+#define MDPD_IN(i, n) ::mdpd::index_ok((i), (n), &B.st->status)
+#else
+#define MDPD_IDX(i, n) (i)
+#define MDPD_IN(i, n) true
+#endif
+
+// locals plus the ghost images of the last build: the bound of a neighbour index
+__host__ __device__ __forceinline__ int n_all(const BoxDesc &B)
+{
+    return B.nlocal + (B.st->nghost < B.ghost_cap ? B.st->nghost : B.ghost_cap);
 }
 
 // entry k of particle i in the locally transposed table

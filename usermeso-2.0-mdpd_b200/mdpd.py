@@ -83,6 +83,7 @@ def lib():
             "mdpd_geometry": ([vp, dp], C.c_int),
             "mdpd_get_pairs": ([vp, i32p, i32p, i64, C.POINTER(i64)], C.c_int),
             "mdpd_gaussian": ([u32p, u32p, dp, fp, i64], C.c_int),
+            "mdpd_index_checks": ([], C.c_int),
             "mdpd_batch_create": ([C.POINTER(vp), C.POINTER(BoxSpec), i32, C.POINTER(Opts)], C.c_int),
             "mdpd_batch_setup": ([vp], C.c_int), "mdpd_batch_step": ([vp, i64], C.c_int),
             "mdpd_batch_thermo": ([vp, i32, C.POINTER(Thermo)], C.c_int),
@@ -224,6 +225,11 @@ class Lammps:
             self.close()
         except Exception:
             pass
+
+
+def index_checks():
+    """True when the loaded library is the index-check build (libmdpd_check.so, MDPD_LIB)."""
+    return lib().mdpd_index_checks() == 1
 
 
 def gaussian(si, sj, exact=True, fast=True):
