@@ -153,6 +153,17 @@ int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int
  * warp shares its 32 particles' pairs; fixed). Full-list batches (classic DPD, wall-coupled
  * mDPD): threads per particle of the density and force passes (1, 2 or 4 each). */
 int mdpd_batch_tune(mdpd_batch_t *b, int32_t *shape_density, int32_t *shape_force);
+/* mdpd_batch_tune with its picks persisted in a JSON file (path; created when absent):
+ * {"version": 1, "entries": {"<key>": {"density": D, "force": F, "ms_per_step": T}}}.  The key
+ * names the workload class the pick applies to: GPU model and SM count, pass family and options,
+ * mean density (0.25 steps), neighbour cutoff (0.05 steps), total particles and box count (powers
+ * of two).  A stored key is applied without stepping the boxes (*cached = 1); otherwise the batch
+ * is timed as by mdpd_batch_tune and its pick added to the file (*cached = 0), which is rewritten
+ * whole through a temporary and a rename, keeping the other members.  A malformed file or entry
+ * returns MDPD_ERR_PARSE and is left untouched.  The reference's ThreadTuner learns online and
+ * keeps nothing across runs (autotuner_meso.h:11-96). */
+int mdpd_batch_tune_cached(mdpd_batch_t *b, const char *path, int32_t *shape_density, int32_t *shape_force,
+                           int32_t *cached);
 /* last per-step device time in milliseconds measured with CUDA events over nsteps */
 int mdpd_batch_time(mdpd_batch_t *b, int64_t nsteps, double *ms_per_step);
 /* nsteps un-captured steps with CUDA events around each kernel group (same kernels as the

@@ -1,6 +1,7 @@
 """Batched and served boxes: each box's result is bitwise the same alone and in the mix
 (counter-based RNG, per-box deterministic lists and reductions); admission honours the
 HBM budget; failures of one job leave the others' results unchanged."""
+import json
 import time
 
 import numpy as np
@@ -172,3 +173,37 @@ def test_server_preempt_checkpoint_and_resume():
     dx = np.mod(xr - xe + L / 2, L) - L / 2
     assert np.abs(dx).max() < 1e-2
 
+
+
+def test_tune_cache_persists_the_pick(tmp_path):
+    cache = tmp_path / "tune.json"
+    sp = specs()
+    b = mdpd.Batch(sp)
+    b.setup()
+    d, f, hit = b.tune(cache=cache)
+    assert not hit and d in (4, 6, 8) and f == 32
+    assert b.thermo(0).step == 39  # three candidates, 13 timed steps each
+    doc = json.loads(cache.read_text())
+    (key, entry), = doc["entries"].items()
+    assert "pair-once" in key and entry["density"] == d and entry["ms_per_step"] > 0
+    b.close()
+    # a batch of the same workload class takes the stored pick without stepping, and steps as a
+    # batch configured by timing does
+    b2 = mdpd.Batch(sp)
+    b2.setup()
+    assert b2.tune(cache=cache) == (d, f, True)
+    assert b2.thermo(0).step == 0
+    b2.step(30)
+    assert b2.thermo(0).status == 0 and b2.thermo(0).step == 30
+    b2.close()
+    # a stored shape the family does not offer is refused, the file left as it was
+    doc["entries"][key]["density"] = 5
+    cache.write_text(json.dumps(doc))
+    before = cache.read_text()
+    b3 = mdpd.Batch(sp)
+    b3.setup()
+    with pytest.raises(mdpd.MdpdError) as e:
+        b3.tune(cache=cache)
+    assert e.value.code == mdpd.ERR_PARSE and "does not offer" in str(e.value)
+    assert cache.read_text() == before
+    b3.close()

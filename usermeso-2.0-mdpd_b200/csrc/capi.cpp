@@ -3,6 +3,7 @@
 // mdpd_last_error.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <random>
@@ -12,6 +13,7 @@
 #include "../../include/mdpd.h"
 #include "engine.h"
 #include "script.h"
+#include "tune_cache.h"
 
 using namespace mdpd;
 
@@ -553,48 +555,137 @@ int mdpd_batch_time(mdpd_batch_t *b, int64_t nsteps, double *ms)
     });
 }
 
+// candidate shapes of the pair passes for the batch's pass family
+static std::vector<StepConfig> tune_candidates(const StepConfig &base)
+{
+    std::vector<StepConfig> cands;
+    if (base.half) {  // pair-once passes: the density pass's gathers in flight
+        for (int g : {4, 6, 8}) {
+            StepConfig c = base;
+            c.gather = g;
+            cands.push_back(c);
+        }
+    } else {  // full-list passes: threads per particle of each pass
+        for (int td : {1, 2, 4})
+            for (int tf : {1, 2, 4}) {
+                StepConfig c = base;
+                c.tpp_density = td;
+                c.tpp_force = tf;
+                cands.push_back(c);
+            }
+    }
+    return cands;
+}
+
+static TunePick pick_of(const StepConfig &c, double ms)
+{
+    TunePick p;
+    p.density = c.half ? c.gather : c.tpp_density;
+    p.force = c.half ? 32 : c.tpp_force;
+    p.ms_per_step = ms;
+    return p;
+}
+
+// time every candidate on the batch (3 + 10 real steps each) and keep the fastest
+static TunePick tune_by_timing(mdpd_batch_s *b)
+{
+    const StepConfig base = b->batch->cfg;
+    double best = 1e30;
+    StepConfig pick = base;
+    for (const StepConfig &c : tune_candidates(base)) {
+        b->batch->reconfigure(c);
+        b->batch->run(3, true);
+        cudaEvent_t e0, e1;
+        check_cuda(cudaEventCreate(&e0), "event");
+        check_cuda(cudaEventCreate(&e1), "event");
+        cudaEventRecord(e0, b->batch->stream());
+        b->batch->run(10, false);
+        cudaEventRecord(e1, b->batch->stream());
+        cudaEventSynchronize(e1);
+        float t = 0;
+        cudaEventElapsedTime(&t, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (t < best) best = t, pick = c;
+    }
+    b->batch->reconfigure(pick);
+    return pick_of(pick, best / 10.0);
+}
+
+// the workload class a stored pick applies to: GPU model and SM count, the pass family and
+// its options, mean density (0.25 steps), neighbour cutoff (0.05 steps), total particles and
+// box count (powers of two)
+static std::string tune_key(mdpd_batch_s *b)
+{
+    const Batch &bt = *b->batch;
+    const StepConfig &c = bt.cfg;
+    cudaDeviceProp prop{};
+    check_cuda(cudaGetDeviceProperties(&prop, b->device), "device properties");
+    long long ntot = 0;
+    double vol = 0.0, rc = 0.0;
+    for (Box *x : bt.boxes()) {
+        ntot += x->n;
+        vol += x->desc.prd[0] * x->desc.prd[1] * x->desc.prd[2];
+        rc = std::max(rc, x->desc.cutghost);
+    }
+    std::string fam = c.half ? "mdpd pair-once" : c.style ? "dpd full-list" : "mdpd full-list";
+    if (c.wall_coupling) fam += " +wall-coupling";
+    if (c.wall) fam += " +bounce-back";
+    if (c.aboundary) fam += " +aboundary";
+    if (c.exact_rng) fam += " +exact-rng";
+    if (!c.uniform_types) fam += " +types";
+    const int nb = (int)bt.boxes().size();
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "%s sm%d | %s | rho %.2f | rc %.2f | particles 2^%d | boxes 2^%d", prop.name,
+                  prop.multiProcessorCount, fam.c_str(), std::round(4.0 * ntot / std::max(vol, 1e-300)) / 4.0,
+                  std::round(20.0 * rc) / 20.0, ntot > 0 ? (int)std::floor(std::log2((double)ntot)) : 0,
+                  (int)std::floor(std::log2((double)std::max(nb, 1))));
+    return buf;
+}
+
 int mdpd_batch_tune(mdpd_batch_t *b, int32_t *shape_density, int32_t *shape_force)
 {
     if (!b) return MDPD_ERR_ARG;
     return guard(b->err, [&] {
+        const TunePick p = tune_by_timing(b);
+        if (shape_density) *shape_density = p.density;
+        if (shape_force) *shape_force = p.force;
+        std::string msg;
+        if (int st = b->batch->status(msg)) throw ScriptError(st & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, msg);
+    });
+}
+
+int mdpd_batch_tune_cached(mdpd_batch_t *b, const char *path, int32_t *shape_density, int32_t *shape_force,
+                           int32_t *cached)
+{
+    if (!b || !path || !*path) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        const std::string key = tune_key(b);
         const StepConfig base = b->batch->cfg;
-        std::vector<StepConfig> cands;
-        if (base.half) {  // pair-once passes: the density pass's gathers in flight
-            for (int g : {4, 6, 8}) {
-                StepConfig c = base;
-                c.gather = g;
-                cands.push_back(c);
-            }
-        } else {  // full-list passes: threads per particle of each pass
-            for (int td : {1, 2, 4})
-                for (int tf : {1, 2, 4}) {
-                    StepConfig c = base;
-                    c.tpp_density = td;
-                    c.tpp_force = tf;
-                    cands.push_back(c);
+        TunePick p;
+        const bool hit = tune_cache_get(path, key, p);
+        if (hit) {
+            // the stored shapes must be ones this batch's family offers
+            const StepConfig *use = nullptr;
+            for (const StepConfig &c : tune_candidates(base)) {
+                const TunePick q = pick_of(c, 0.0);
+                if (q.density == p.density && q.force == p.force) {
+                    b->batch->reconfigure(c);
+                    use = &c;
+                    break;
                 }
+            }
+            if (!use)
+                throw std::runtime_error("PARSE: tune cache " + std::string(path) + ": entry \"" + key +
+                                         "\" holds shapes (" + std::to_string(p.density) + ", " +
+                                         std::to_string(p.force) + ") this pass family does not offer");
+        } else {
+            p = tune_by_timing(b);
+            tune_cache_put(path, key, p);
         }
-        double best = 1e30;
-        StepConfig pick = base;
-        for (const StepConfig &c : cands) {
-            b->batch->reconfigure(c);
-            b->batch->run(3, true);
-            cudaEvent_t e0, e1;
-            check_cuda(cudaEventCreate(&e0), "event");
-            check_cuda(cudaEventCreate(&e1), "event");
-            cudaEventRecord(e0, b->batch->stream());
-            b->batch->run(10, false);
-            cudaEventRecord(e1, b->batch->stream());
-            cudaEventSynchronize(e1);
-            float t = 0;
-            cudaEventElapsedTime(&t, e0, e1);
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            if (t < best) best = t, pick = c;
-        }
-        b->batch->reconfigure(pick);
-        if (shape_density) *shape_density = base.half ? pick.gather : pick.tpp_density;
-        if (shape_force) *shape_force = base.half ? 32 : pick.tpp_force;
+        if (shape_density) *shape_density = p.density;
+        if (shape_force) *shape_force = p.force;
+        if (cached) *cached = hit ? 1 : 0;
         std::string msg;
         if (int st = b->batch->status(msg)) throw ScriptError(st & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, msg);
     });

@@ -89,6 +89,7 @@ def lib():
             "mdpd_batch_thermo": ([vp, i32, C.POINTER(Thermo)], C.c_int),
             "mdpd_batch_get_state": ([vp, i32, dp, dp, i64], C.c_int),
             "mdpd_batch_tune": ([vp, i32p, i32p], C.c_int),
+            "mdpd_batch_tune_cached": ([vp, cp, i32p, i32p, i32p], C.c_int),
             "mdpd_batch_time": ([vp, i64, dp], C.c_int),
             "mdpd_batch_profile": ([vp, i64, dp], C.c_int),
             "mdpd_batch_rebuild_steps": ([vp, C.POINTER(i64)], C.c_int),
@@ -310,10 +311,17 @@ class Batch:
         self._check(lib().mdpd_batch_rebuild_steps(self.h, C.byref(n)))
         return n.value
 
-    def tune(self):
+    def tune(self, cache=None):
+        """pair-pass shapes (density, force) picked by timing the batch; with cache (a JSON file
+        path) a stored pick for this workload class is applied without stepping.  With cache the
+        result is (density, force, cached)."""
         a, b = C.c_int32(), C.c_int32()
-        self._check(lib().mdpd_batch_tune(self.h, C.byref(a), C.byref(b)))
-        return a.value, b.value
+        if cache is None:
+            self._check(lib().mdpd_batch_tune(self.h, C.byref(a), C.byref(b)))
+            return a.value, b.value
+        hit = C.c_int32()
+        self._check(lib().mdpd_batch_tune_cached(self.h, os.fsencode(cache), C.byref(a), C.byref(b), C.byref(hit)))
+        return a.value, b.value, bool(hit.value)
 
     def thermo(self, box):
         t = Thermo()
