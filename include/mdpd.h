@@ -213,6 +213,22 @@ int mdpd_server_cancel(mdpd_server_t *s, int64_t job_id);
  * dissipative force then sees v at the full step once, where the running job had the half
  * step, so the continuation is statistically, not bitwise, the uninterrupted run) */
 int mdpd_server_preempt(mdpd_server_t *s, int64_t job_id);
+/* JSON job specs: a file of boxes for one server,
+ *   {"budget_gb": G, "timeout_s": T, "defaults": {<key>: value, ...},
+ *    "jobs": [{"name": "a", "n": N, "box": L or [Lx, Ly, Lz], "steps": S, <key>: value, ...}]}
+ * with a key per mdpd_box_spec field (style "mdpd"|"dpd", lo, A, B, gamma, kT, cut, cut_r,
+ * cut_rho, sigma, dt, skin, rho_est, mass, seed, every, delay, check, exact_rng, init_seed,
+ * fill_lo, fill_hi, start_step; unset ones take the mdpd/meso deck defaults).  An unknown key, a
+ * value of the wrong kind, a missing n/box/steps or a box above the budget is MDPD_ERR_PARSE
+ * naming the job and key, reported before any device work.
+ * mdpd_jobs_validate: checks the file; the job count and the summed device footprint.
+ * mdpd_run_jobs: submits every job to one server and waits for them (timeout_s, 0: no limit),
+ * then writes to out_path (NULL: stdout) one JSON line per job in file order (state, steps,
+ * queue and run seconds, particle-steps/s, p50/p99 step ms, builds, final temp/pe/press, status)
+ * and a {"summary": ...} line with the server counters; returns the MDPD_* code of the first
+ * job that did not finish, or MDPD_OK. */
+int mdpd_jobs_validate(const char *spec_path, int32_t *njobs, uint64_t *bytes);
+int mdpd_run_jobs(const char *spec_path, const char *out_path, const mdpd_opts *opts);
 /* wait until every submitted job is done, failed or cancelled (timeout_s <= 0: no limit) */
 int mdpd_server_drain(mdpd_server_t *s, double timeout_s);
 /* throughput/latency summary: particle-steps/s, step p50/p99 ms, job p50/p99 s,

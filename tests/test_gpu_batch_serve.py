@@ -207,3 +207,53 @@ def test_tune_cache_persists_the_pick(tmp_path):
     assert e.value.code == mdpd.ERR_PARSE and "does not offer" in str(e.value)
     assert cache.read_text() == before
     b3.close()
+
+
+def test_json_job_spec_runs_on_the_server(tmp_path):
+    spec = {
+        "budget_gb": 0.012,  # 12.9 MB: b (9.5 MB) alone, or a + dpd (11.6 MB) by size alone
+        "jobs": [
+            {"name": "a", "n": 3000, "box": 8.0, "steps": 60, "seed": 3, "init_seed": 5},
+            # fits beside a, but a DPD box steps with other kernels: it waits until a has ended
+            {"name": "dpd", "style": "dpd", "n": 3000, "box": 8.0, "A": 25, "sigma": 3.0, "steps": 30},
+            {"name": "b", "n": 5000, "box": [12, 8, 8], "steps": 40, "seed": 4, "init_seed": 6},
+        ],
+    }
+    p = tmp_path / "jobs.json"
+    p.write_text(json.dumps(spec))
+    n, foot = mdpd.validate_jobs(p)
+    assert n == 3 and foot > 0
+    lines = mdpd.run_jobs(p, tmp_path / "out.jsonl")
+    jobs, summary = lines[:-1], lines[-1]["summary"]
+    assert [j["job"] for j in jobs] == ["a", "dpd", "b"]
+    for j, s in zip(jobs, spec["jobs"]):
+        assert j["state"] == "done" and j["error"] == 0 and j["status"] == 0, j
+        assert j["steps_done"] == s["steps"] and j["n"] == s["n"]
+        assert j["nbuild"] > 0 and j["temp"] > 0 and j["particle_steps_per_s"] > 0
+        assert j["step_ms_p99"] >= j["step_ms_p50"] > 0
+    assert summary["done"] == 3 and summary["jobs"] == 3
+    assert 0 < summary["peak_resident_bytes"] <= 0.012 * 2 ** 30
+    assert jobs[1]["queue_s"] >= jobs[0]["run_s"] * 0.5  # the DPD job did not join a
+    # the same jobs through the Python spec builder, each in a batch of its own, end in the same state
+    for k, sp in ((0, mdpd.box_spec(3000, 8.0, seed=3, init_seed=5)),
+                  (1, mdpd.box_spec(3000, 8.0, style=1, A=25, sigma=3.0))):
+        alone = run_alone(sp, spec["jobs"][k]["steps"])
+        assert alone[2].temp == jobs[k]["temp"] and alone[2].nbuild == jobs[k]["nbuild"], k
+
+
+def test_server_keeps_pass_families_apart():
+    # an exact-RNG job and a DPD job submitted beside a default mDPD job: each ends as it does alone
+    sp = [mdpd.box_spec(2500, 7.5, seed=11, init_seed=2), mdpd.box_spec(2500, 7.5, seed=12, init_seed=3, exact_rng=1),
+          mdpd.box_spec(2500, 7.5, style=1, A=25, seed=13, init_seed=4)]
+    alone = [run_alone(s, 40) for s in sp]
+    srv = mdpd.Server(budget_bytes=int(2e9))
+    ids = [srv.submit(s, 40, keep_state=True) for s in sp]
+    srv.drain(timeout_s=300)
+    for k, jid in enumerate(ids):
+        assert srv.poll(jid).state == 2
+        x, v = srv.state(jid, sp[k].n)
+        assert np.array_equal(x, alone[k][0]) and np.array_equal(v, alone[k][1]), k
+    srv.stop()
+    with pytest.raises(mdpd.MdpdError) as e:
+        mdpd.Batch(sp[:2])
+    assert e.value.code == mdpd.ERR_ARG and "RNG mode" in str(e.value)

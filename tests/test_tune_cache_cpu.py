@@ -1,6 +1,6 @@
-"""The persisted autotuner store (csrc/tune_cache.cpp) on the host: no GPU.
+"""The persisted autotuner store (csrc/tune_cache.cpp, on csrc/json.cpp) on the host: no GPU.
 
-A small C++ driver compiled with g++ against tune_cache.cpp stores and reads picks:
+A small C++ driver compiled with g++ against tune_cache.cpp and json.cpp stores and reads picks:
 round trip, a second key merged beside the first, a key replaced, members the store does
 not own kept on rewrite, keys with quotes and backslashes, a missing file as a miss, and a
 malformed file or entry refused with the PARSE prefix and left byte for byte as it was.
@@ -52,7 +52,7 @@ def driver(tmp_path_factory):
     src.write_text(DRIVER)
     exe = d / "driver"
     subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-I" + CSRC, str(src), os.path.join(CSRC, "tune_cache.cpp"),
-                    "-o", str(exe)], check=True, capture_output=True, text=True)
+                    os.path.join(CSRC, "json.cpp"), "-o", str(exe)], check=True, capture_output=True, text=True)
 
     def run(*args):
         r = subprocess.run([str(exe)] + [str(a) for a in args], capture_output=True, text=True, check=True)

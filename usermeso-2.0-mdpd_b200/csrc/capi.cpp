@@ -5,6 +5,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <iostream>
 #include <memory>
 #include <random>
 #include <stdexcept>
@@ -12,6 +14,7 @@
 
 #include "../../include/mdpd.h"
 #include "engine.h"
+#include "jobs.h"
 #include "script.h"
 #include "tune_cache.h"
 
@@ -447,6 +450,8 @@ int mdpd_batch_create(mdpd_batch_t **out, const mdpd_box_spec *specs, int32_t nb
         try {
             for (int k = 0; k < nbox; ++k) {
                 if (specs[k].style != cfg.style) throw std::runtime_error("ARG: a batch holds boxes of one pair style");
+                if ((specs[k].exact_rng != 0) != (cfg.exact_rng != 0))
+                    throw std::runtime_error("ARG: a batch holds boxes of one RNG mode (exact_rng)");
                 Spec s;
                 Particles p;
                 spec_from_box(specs[k], s, p);
@@ -688,6 +693,39 @@ int mdpd_batch_tune_cached(mdpd_batch_t *b, const char *path, int32_t *shape_den
         if (cached) *cached = hit ? 1 : 0;
         std::string msg;
         if (int st = b->batch->status(msg)) throw ScriptError(st & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, msg);
+    });
+}
+
+int mdpd_jobs_validate(const char *spec_path, int32_t *njobs, uint64_t *bytes)
+{
+    if (!spec_path) return MDPD_ERR_ARG;
+    return guard(g_err, [&] {
+        const JobFile jf = read_job_file(spec_path);
+        uint64_t total = 0;
+        for (const JobEntry &e : jf.jobs) {
+            uint64_t b = 0;
+            mdpd_box_bytes(&e.spec.box, &b);
+            total += b;
+        }
+        if (njobs) *njobs = (int32_t)jf.jobs.size();
+        if (bytes) *bytes = total;
+    });
+}
+
+int mdpd_run_jobs(const char *spec_path, const char *out_path, const mdpd_opts *opts)
+{
+    if (!spec_path) return MDPD_ERR_ARG;
+    return guard(g_err, [&] {
+        const JobFile jf = read_job_file(spec_path);  // every job checked before the device is touched
+        int rc;
+        if (out_path && *out_path) {
+            std::ofstream f(out_path, std::ios::binary | std::ios::trunc);
+            if (!f) throw std::runtime_error("ARG: cannot write " + std::string(out_path));
+            rc = run_job_file(jf, opts, f);
+        } else {
+            rc = run_job_file(jf, opts, std::cout);
+        }
+        if (rc) throw ScriptError(rc, "a job did not finish (MDPD_* code " + std::to_string(rc) + "): see its result line");
     });
 }
 

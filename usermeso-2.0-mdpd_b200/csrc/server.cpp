@@ -82,6 +82,13 @@ struct mdpd_server_s {
     void loop();
 };
 
+// the kernels of a batch are chosen per batch (pair style, RNG mode): jobs step together only
+// when they share both
+static bool same_family(const Job &a, const Job &b)
+{
+    return a.spec.box.style == b.spec.box.style && (a.spec.box.exact_rng != 0) == (b.spec.box.exact_rng != 0);
+}
+
 void mdpd_server_s::loop()
 {
     cudaSetDevice(device);
@@ -116,6 +123,9 @@ void mdpd_server_s::loop()
                     continue;
                 }
                 if (resident + j->bytes > budget) break;
+                // another pass family waits, in order, until the resident jobs have ended
+                const Job *ref = !active.empty() ? active[0].get() : !admitted.empty() ? admitted[0].get() : nullptr;
+                if (ref && !same_family(*j, *ref)) break;
                 queue.pop_front();
                 resident += j->bytes;
                 admitted.push_back(j);
@@ -157,6 +167,7 @@ void mdpd_server_s::loop()
             std::vector<Box *> raw;
             for (auto &j : active) raw.push_back(j->box.get());
             cfg.style = active[0]->spec.box.style;
+            cfg.exact_rng = active[0]->spec.box.exact_rng != 0;
             try {
                 batch.reset(new Batch(raw, cfg));
                 for (size_t k = 0; k < active.size(); ++k)

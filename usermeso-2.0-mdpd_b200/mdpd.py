@@ -84,6 +84,8 @@ def lib():
             "mdpd_get_pairs": ([vp, i32p, i32p, i64, C.POINTER(i64)], C.c_int),
             "mdpd_gaussian": ([u32p, u32p, dp, fp, i64], C.c_int),
             "mdpd_index_checks": ([], C.c_int),
+            "mdpd_jobs_validate": ([cp, i32p, C.POINTER(C.c_uint64)], C.c_int),
+            "mdpd_run_jobs": ([cp, cp, C.POINTER(Opts)], C.c_int),
             "mdpd_batch_create": ([C.POINTER(vp), C.POINTER(BoxSpec), i32, C.POINTER(Opts)], C.c_int),
             "mdpd_batch_setup": ([vp], C.c_int), "mdpd_batch_step": ([vp, i64], C.c_int),
             "mdpd_batch_thermo": ([vp, i32, C.POINTER(Thermo)], C.c_int),
@@ -226,6 +228,31 @@ class Lammps:
             self.close()
         except Exception:
             pass
+
+
+def validate_jobs(path):
+    """check a JSON job spec without touching the device: (number of jobs, summed device bytes)"""
+    n, b = C.c_int32(), C.c_uint64()
+    rc = lib().mdpd_jobs_validate(os.fsencode(path), C.byref(n), C.byref(b))
+    if rc:
+        raise MdpdError(rc, lib().mdpd_last_error(None).decode())
+    return n.value, b.value
+
+
+def run_jobs(path, out_path, device=0):
+    """run a JSON job spec on the serving loop; the result lines (one dict per job, then the
+    summary) are written to out_path and returned.  A job that did not finish raises MdpdError
+    after the lines are written."""
+    import json
+    o = Opts(device, 0)
+    rc = lib().mdpd_run_jobs(os.fsencode(path), os.fsencode(out_path), C.byref(o))
+    if rc and not os.path.exists(out_path):
+        raise MdpdError(rc, lib().mdpd_last_error(None).decode())
+    with open(out_path) as f:
+        lines = [json.loads(t) for t in f if t.strip()]
+    if rc:
+        raise MdpdError(rc, lib().mdpd_last_error(None).decode() + "\n" + "\n".join(map(str, lines)))
+    return lines
 
 
 def index_checks():
