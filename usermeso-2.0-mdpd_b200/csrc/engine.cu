@@ -210,6 +210,7 @@ void Box::layout(const Spec &s, int na)
 
 Box::Box(const Spec &s, const Particles &p, int sms) : spec(s)
 {
+    Range r("mdpd::box_create");
     (void)sms;
     n = (int)p.size();
     try {
@@ -224,6 +225,7 @@ Box::Box(const Spec &s, int n_, const double *x, const double *v, const int32_t 
          const int32_t *mask, int sms, bool wait)
     : spec(s)
 {
+    Range r("mdpd::box_create");
     (void)sms;
     n = n_;
     try {
@@ -405,6 +407,7 @@ void Box::release() noexcept
 
 void Box::download_by_tag(double *x, double *v, double *scratch) const
 {
+    Range r("mdpd::download");
     const BoxState st = state();
     const int c = st.cur;
     double *d = scratch;
@@ -552,6 +555,7 @@ void Batch::build_units()
 
 void Batch::capture(int ev)
 {
+    Range r("mdpd::capture");
     cudaGraph_t g;
     check_cuda(cudaGraphCreate(&g, 0), "graph create");
     cudaGraphConditionalHandle h;
@@ -591,6 +595,7 @@ void Batch::capture(int ev)
 
 void Batch::setup()
 {
+    Range r("mdpd::setup");
     launch_force_rebuild_flag(stream_, d_boxes, units.nbox, 1);
     launch_rebuild(stream_, d_boxes, units, cfg, d_done);
     if (cfg.style == 0) launch_density(stream_, d_boxes, units, cfg);
@@ -612,6 +617,7 @@ __global__ void k_set_rebuild(BoxDesc *boxes, const int *which, int nwhich, int 
 
 void Batch::setup_boxes(const std::vector<int> &which)
 {
+    Range r("mdpd::setup");
     if (which.empty()) return;
     int *d = nullptr;
     check_cuda(cudaMallocAsync(&d, sizeof(int) * which.size(), stream_), "setup boxes");
@@ -646,6 +652,7 @@ void Batch::reconfigure(const StepConfig &c)
 
 void Batch::run(long long nsteps, bool sync)
 {
+    Range r("mdpd::run");
     for (long long k = 0; k < nsteps; ++k) check_cuda(cudaGraphLaunch(graph_[0], stream_), "graph launch");
     if (sync) check_cuda(cudaStreamSynchronize(stream_), "run");
 }
@@ -667,14 +674,26 @@ void Batch::profile(long long nsteps, double out[5])
     const long long r0 = rebuild_steps();
     for (long long k = 0; k < nsteps; ++k) {
         cudaEventRecord(ev[0], stream_);
-        launch_integrate(stream_, d_boxes, units, cfg, d_done, cudaGraphConditionalHandle{}, 0);
+        {
+            Range r("integrate");
+            launch_integrate(stream_, d_boxes, units, cfg, d_done, cudaGraphConditionalHandle{}, 0);
+        }
         cudaEventRecord(ev[1], stream_);
-        launch_rebuild(stream_, d_boxes, units, cfg, d_done);  // kernels skip boxes not rebuilding
+        {
+            Range r("rebuild");
+            launch_rebuild(stream_, d_boxes, units, cfg, d_done);  // kernels skip boxes not rebuilding
+        }
         cudaEventRecord(ev[2], stream_);
-        if (cfg.style == 0) launch_density(stream_, d_boxes, units, cfg);
+        if (cfg.style == 0) {
+            Range r("density");
+            launch_density(stream_, d_boxes, units, cfg);
+        }
         cudaEventRecord(ev[3], stream_);
-        launch_force(stream_, d_boxes, units, cfg, 0, 1);
-        if (cfg.aboundary) launch_aboundary_meso(stream_, d_boxes, units);
+        {
+            Range r("force");
+            launch_force(stream_, d_boxes, units, cfg, 0, 1);
+            if (cfg.aboundary) launch_aboundary_meso(stream_, d_boxes, units);
+        }
         cudaEventRecord(ev[4], stream_);
         check_cuda(cudaEventSynchronize(ev[4]), "profile");
         for (int q = 0; q < 4; ++q) {
@@ -690,6 +709,7 @@ void Batch::profile(long long nsteps, double out[5])
 
 void Batch::thermo(std::vector<Thermo> &out)
 {
+    Range r("mdpd::thermo");
     launch_thermo(stream_, d_boxes, units, d_thermo, d_done + 2);
     check_cuda(cudaGetLastError(), "thermo launch");
     const int nb = (int)boxes_.size();

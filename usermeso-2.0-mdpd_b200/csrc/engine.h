@@ -2,6 +2,7 @@
 // boxes stepped by one captured CUDA graph per step, thermo reductions.
 #pragma once
 
+#include <nvtx3/nvToolsExt.h>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -145,6 +146,16 @@ private:
     cudaGraph_t graph_src_[2] = {nullptr, nullptr};
     void build_units();
     void capture(int ev);
+};
+
+// an NVTX range over a host scope: the phases of setup, stepping, rebuild and I/O show by name on
+// an Nsight timeline, and `ncu --nvtx --nvtx-include "<name>/"` selects the kernels launched in
+// one (a push and a pop, nanoseconds, when no tool is attached)
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
 };
 
 std::string status_text(int bits);  // names of the set bits of a box status word

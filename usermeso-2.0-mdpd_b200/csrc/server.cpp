@@ -192,6 +192,7 @@ void mdpd_server_s::loop()
         int64_t k = chunk;
         for (auto &j : active) k = std::min<int64_t>(k, j->spec.nsteps - j->done);
         k = std::max<int64_t>(k, 1);
+        Range chunk_range("mdpd::server_chunk");
         cudaEventRecord(e0, batch->stream());
         batch->run(k, false);
         cudaEventRecord(e1, batch->stream());
