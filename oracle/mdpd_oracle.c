@@ -706,7 +706,7 @@ void orc_force_mdpd(int nlocal, const float *pos4, const float *vel4, const doub
                 h *= c->cut;
                 double q = 1.0 - h / c->cut;
                 double ratio = 1.0 + 0.187 * (c->cut / h - 1.0) - 0.093 * q * q * q;
-                sig *= sqrt(ratio);
+                sig *= (double)sqrtf((float)ratio); /* sqrtf: FP32, as pair_mdpd_meso.cu:181 */
                 gam *= ratio;
             }
             double fp = (c->A * wc + c->B * (rho[i] + rho[j]) * wcr) - gam * wc * wc * dot * rinv +
