@@ -53,6 +53,7 @@ def test_validate_counts_jobs_and_footprint(tmp_path):
     (lambda d: d["defaults"].update(gama=4.5), 'defaults: unknown key "gama"'),
     (lambda d: d.update(budget_gb=0.01), "above budget_gb"),
     (lambda d: d.update(jobs=[]), '"jobs" must list at least one job'),
+    (lambda d: d["jobs"][0].update(cut=0.7), "job 0 (small): PARSE: cutA should be larger than cutB"),
 ])
 def test_bad_specs_name_the_job_and_key(tmp_path, edit, words):
     doc = json.loads(json.dumps(SPEC))

@@ -19,9 +19,12 @@
 #include <sstream>
 #include <stdexcept>
 
+#include "engine.h"
 #include "json.h"
 
 namespace mdpd {
+
+void spec_from_box(const mdpd_box_spec &bs, Spec &s, Particles &p);  // capi.cpp
 
 namespace {
 
@@ -182,7 +185,16 @@ JobFile read_job_file(const std::string &path)
         for (auto &o : jf.jobs)
             if (o.name == e.name) bad(path, where, "duplicate name \"" + e.name + "\"");
         uint64_t bytes = 0;
-        if (mdpd_box_bytes(&b, &bytes) != MDPD_OK) bad(path, where, "box parameters rejected (mdpd_box_bytes)");
+        try {  // the checks a box of this spec meets at creation, with their messages
+            Spec sp;
+            Particles p;
+            mdpd_box_spec one = b;
+            one.n = 1;
+            spec_from_box(one, sp, p);
+            bytes = Box::estimate_bytes(sp, b.n);
+        } catch (const std::exception &ex) {
+            bad(path, where, ex.what());
+        }
         if (bytes > jf.budget_bytes)
             bad(path, where, "needs " + std::to_string(bytes) + " device bytes, above budget_gb");
         jf.jobs.push_back(e);
