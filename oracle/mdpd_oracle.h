@@ -1,7 +1,7 @@
 /*
  * CPU oracle for the USER-MESO DPD/mDPD timestep hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker that the CUDA path is
+ * TEST INFRASTRUCTURE ONLY.  This library is the oracle that the CUDA path is
  * compared against, and the CPU baseline timed beside it.  Nothing in the
  * product (libmdpd.so) links, loads or calls it.
  *

@@ -1,6 +1,6 @@
 """ctypes front of the CPU oracle (liboracle.so) -- TEST INFRASTRUCTURE ONLY.
 
-Used by tests/, __graft_entry__.smoke() and bench.py's CPU baseline legs as the checker
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU baseline legs as the oracle
 and as the timed CPU restatement; never by the product library.  Each helper runs the
 reference's algorithm for one hot-path function (see mdpd_oracle.h for file:line).
 """

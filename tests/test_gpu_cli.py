@@ -33,7 +33,7 @@ run 40
 
 @pytest.fixture(scope="module")
 def lmp():
-    if not os.path.exists(LMP):  # the driver is built beside libmdpd.so
+    if not os.path.exists(LMP):  # the command-line program is built beside libmdpd.so
         sys.path.insert(0, PKG)
         import build
         build.build(verbose=False)

@@ -1,6 +1,6 @@
 """The oracle's rebuild (oracle.rebuild: pbc wrap, 2-level reorder sort, ghost images, FP32 pack,
 full neighbour list) against independent numpy restatements, so the bit-exact GPU parity tests
-that compare with it stand on a checked checker.  No GPU.
+that compare with it stand on a checked oracle.  No GPU.
 
 1. Sort permutation: the reorder key of gpu_build_reorder_keypair<1> (atom_meso.cu:271-311)
    with MesoAtom::sort_local's widths (atom_meso.cu:346-387), border slabs of MesoComm::borderness

@@ -1,6 +1,6 @@
 """The oracle's restatements of the pair-once rows (orc_reduce_rows) and of fix aboundary/meso
 (orc_aboundary_meso) against independent numpy ones, so the GPU parity tests that lean on them
-stand on a checked checker. No GPU.
+stand on a checked oracle. No GPU.
 
 numpy has no fused multiply-add: fmaf(a, b, c) is emulated by rounding a*b + c, taken in FP64
 (a*b of two FP32 values is exact there), to FP32. That double rounding can differ from fmaf in
