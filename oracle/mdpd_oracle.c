@@ -453,8 +453,9 @@ void orc_reduce_rows(int nlocal, int ncol, const int32_t *count, const int32_t *
 /* fix aboundary/meso at the end of a step (gpu_aboundary_v2, fix_aboundary_meso.cu:186-281):
  * a particle of the mobile group is projected half a kick and one drift ahead (v + dt/2 f,
  * x + dt v, unit mass as the reference writes it); the Gaussian density of the wall particles
- * among its row's core entries (the first count_core[i], core entries first as the reference
- * joins them) is summed at that point; above rho0/2 the parts of v and f along the direction
+ * of its whole row (count[i] entries: the reference passes dev_pair_count_core, which the list
+ * join gpu_join_neigh_list, neigh_build_meso.cu:188-204, sets to core plus skin) is summed at
+ * that point; above rho0/2 the parts of v and f along the direction
  * into the wall (minus the normalised density gradient) are removed twice over.  FP32 as the
  * reference; its contracted forms are written as fmaf.  v and f (the total force) in place. */
 static float orc_dot3f(float ax, float ay, float az, float bx, float by, float bz)
@@ -462,7 +463,7 @@ static float orc_dot3f(float ax, float ay, float az, float bx, float by, float b
     return fmaf(az, bz, fmaf(ax, bx, ay * by));
 }
 
-void orc_aboundary_meso(int nlocal, const float *pos4, const int32_t *mask_all, const int32_t *count_core,
+void orc_aboundary_meso(int nlocal, const float *pos4, const int32_t *mask_all, const int32_t *count,
                         const int32_t *table, int ncol, int mobile_bit, int wall_bit, double rho0, double sigma,
                         double dt, double *vx, double *vy, double *vz, double *fx, double *fy, double *fz)
 {
@@ -478,7 +479,7 @@ void orc_aboundary_meso(int nlocal, const float *pos4, const int32_t *mask_all, 
         const float cx = fmaf(dtf, px, pos4[4 * i]), cy = fmaf(dtf, py, pos4[4 * i + 1]),
                     cz = fmaf(dtf, pz, pos4[4 * i + 2]);
         float rho = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-        for (int k = 0; k < count_core[i]; ++k) {
+        for (int k = 0; k < count[i]; ++k) {
             const int j = table[(size_t)i * ncol + k];
             if (!(mask_all[j] & wall_bit)) continue;
             const float dx = cx - pos4[4 * j], dy = cy - pos4[4 * j + 1], dz = cz - pos4[4 * j + 2];

@@ -97,7 +97,7 @@ void orc_bin_ids(const orc_box *b, int nlocal, int nall, const double *x, const 
 void orc_reduce_rows(int nlocal, int ncol, const int32_t *count, const int32_t *table,
                      const float *pos4, const int32_t *gimg, float rn2, int32_t *out_count,
                      int32_t *out_table);
-void orc_aboundary_meso(int nlocal, const float *pos4, const int32_t *mask_all, const int32_t *count_core,
+void orc_aboundary_meso(int nlocal, const float *pos4, const int32_t *mask_all, const int32_t *count,
                         const int32_t *table, int ncol, int mobile_bit, int wall_bit, double rho0, double sigma,
                         double dt, double *vx, double *vy, double *vz, double *fx, double *fy, double *fz);
 int orc_build_list(const orc_box *b, int nlocal, int nall, const double *x, const double *y,

@@ -191,12 +191,13 @@ def reduce_rows(count, table, pos4, gimg, rn2):
     return oc, ot
 
 
-def aboundary_meso(pos4, mask_all, count_core, table, mobile_bit, wall_bit, rho0, sigma, dt, v, f):
-    """fix aboundary/meso at the end of a step: returns (v, f) after the wall reflection."""
+def aboundary_meso(pos4, mask_all, count, table, mobile_bit, wall_bit, rho0, sigma, dt, v, f):
+    """fix aboundary/meso at the end of a step over whole rows (count[i] entries): returns (v, f)
+    after the wall reflection."""
     n, ncol = table.shape
     pos4 = np.ascontiguousarray(pos4, np.float32)
     mask_all = np.ascontiguousarray(mask_all, np.int32)
-    cc = np.ascontiguousarray(count_core, np.int32)
+    cc = np.ascontiguousarray(count, np.int32)
     table = np.ascontiguousarray(table, np.int32)
     vv = [np.ascontiguousarray(v[:, d], np.float64).copy() for d in range(3)]
     ff = [np.ascontiguousarray(f[:, d], np.float64).copy() for d in range(3)]

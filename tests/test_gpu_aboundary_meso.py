@@ -5,13 +5,14 @@ A periodic 8 x 8 x 8 box holds a frozen wall slab (z < 2, density 8) and an mDPD
 density threshold) moving into the wall. Two decks differ only in the fix. One step of each (no
 neighbour rebuild in it) gives the state before the fix (the deck without it) and after it (the
 deck with it); the oracle applies its restatement of the fix to the first, over the reference's
-list with its core entries first (oracle rebuild of the same start), and must give the second.
+whole rows (oracle rebuild of the same start: the row length the reference passes is core plus
+skin after its list join), and must give the second.
 
 Tolerances: positions bit-identical (the fix changes v and f only); the set of reflected particles
 identical up to 2 whose wall density lies within FP32 rounding of rho0/2 (CUDA's expf against the
 host's); reflected v and f within 1e-4 of (|v| + 1) and (|f| + 1), the magnitudes before the fix.
 The wall normal is an FP32 sum of Gaussian-weighted offsets that the device takes in its list's
-order and the oracle in the reference's core-first order; its lateral terms largely cancel, so
+order and the oracle in the reference's core-then-skin order; its lateral terms largely cancel, so
 its direction carries a few 1e-5 of relative rounding (a reflection changes v by O(|v|)).
 """
 import numpy as np
@@ -83,7 +84,7 @@ def one_step_parity(nf, nw, x, v, fz=0.0, rho0=8.0):
     n = plain.natoms()
     tags = plain.field("tag")
     assert np.array_equal(tags, ref["tags"]) and np.array_equal(walled.field("tag"), tags)
-    assert plain.thermo().nbuild == 1 and walled.thermo().nbuild == 1  # the setup build: its core entries hold
+    assert plain.thermo().nbuild == 1 and walled.thermo().nbuild == 1  # the setup build's rows
     assert np.array_equal(walled.field("x").view(np.uint64), plain.field("x").view(np.uint64))
     # the state before the fix (internal order), with the oracle's ghosts mapped onto the device's
     pos = plain.field("pos4")
@@ -98,7 +99,7 @@ def one_step_parity(nf, nw, x, v, fz=0.0, rho0=8.0):
     v_pre = vt[tags - 1]
     f_pre = plain.field("force")[:, :3].astype(np.float64)  # the total force, body force included
     sigma = 1.0 / 4.0 / np.pi  # the default rc^2 / (4 pi)
-    v_ref, f_ref = oracle.aboundary_meso(pos, mask_all, ref["count_core"], table, 2, 4, rho0, sigma, 0.01, v_pre, f_pre)
+    v_ref, f_ref = oracle.aboundary_meso(pos, mask_all, ref["count"], table, 2, 4, rho0, sigma, 0.01, v_pre, f_pre)
     _, vw, _, _ = walled.state()
     v_gpu = vw[tags - 1]
     f_gpu = walled.field("force")[:, :3].astype(np.float64)

@@ -57,9 +57,10 @@ def test_reduce_rows_keeps_owned_and_density_range_pairs():
     assert 0.7 * ref["count"].sum() < cnt.sum() < 0.85 * ref["count"].sum()
 
 
-def aboundary_numpy(pos, mask_all, count_core, table, mobile_bit, wall_bit, rho0, sigma, dt, v, f):
-    """fix aboundary/meso (gpu_aboundary_v2, fix_aboundary_meso.cu:186-246) in FP32 numpy"""
-    n = len(count_core)
+def aboundary_numpy(pos, mask_all, count, table, mobile_bit, wall_bit, rho0, sigma, dt, v, f):
+    """fix aboundary/meso (gpu_aboundary_v2, fix_aboundary_meso.cu:186-246) in FP32 numpy, over
+    whole rows: the reference's dev_pair_count_core is core plus skin after the list join"""
+    n = len(count)
     v, f = v.copy(), f.copy()
     sg, r0, dtf = np.float32(sigma), np.float32(rho0), np.float32(dt)
     nf = np.float32(1.0 / np.sqrt((2 * np.pi) ** 3 * sigma ** 3))
@@ -73,7 +74,7 @@ def aboundary_numpy(pos, mask_all, count_core, table, mobile_bit, wall_bit, rho0
         c1 = fmaf(dtf, fmaf(hs, f0, v0), pos[i, :3])
         rho = np.float32(0)
         g = np.zeros(3, np.float32)
-        for j in table[i, :count_core[i]]:
+        for j in table[i, :count[i]]:
             if not mask_all[j] & wall_bit:
                 continue
             d = (c1 - pos[j, :3]).astype(np.float32)
@@ -103,8 +104,8 @@ def test_aboundary_meso_oracle_matches_numpy():
     v = rng.normal(0, 1, (n, 3)) - np.array([0, 0, 1.5])
     f = rng.normal(0, 30, (n, 3))
     sigma = 1.0 / 4.0 / np.pi
-    v_c, f_c = oracle.aboundary_meso(ref["pos4"], mask_all, ref["count_core"], ref["table"], 2, 4, 8.0, sigma, 0.01, v, f)
-    v_n, f_n, rho = aboundary_numpy(ref["pos4"], mask_all, ref["count_core"], ref["table"], 2, 4, 8.0, sigma, 0.01, v, f)
+    v_c, f_c = oracle.aboundary_meso(ref["pos4"], mask_all, ref["count"], ref["table"], 2, 4, 8.0, sigma, 0.01, v, f)
+    v_n, f_n, rho = aboundary_numpy(ref["pos4"], mask_all, ref["count"], ref["table"], 2, 4, 8.0, sigma, 0.01, v, f)
     hit_c = np.any(v_c != v, 1) | np.any(f_c != f, 1)
     hit_n = np.any(v_n != v, 1) | np.any(f_n != f, 1)
     borderline = np.abs(rho - 4.0) <= 1e-5 * 4.0

@@ -269,7 +269,6 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
         B.rn2_list = (float)(rn * rn);
         B.list_reduce = 0;
     }
-    B.rc2_core = (float)std::pow(g.cutneighmax - s.skin, 2.0);  // neigh_build_meso.cu:316-317
     B.ab_mobile_bit = s.ab_mobile_bit;
     B.ab_wall_bit = s.ab_wall_bit;
     B.ab_rho0 = (float)s.ab_rho0;

@@ -229,24 +229,12 @@ void launch_force_rebuild_flag(cudaStream_t s, BoxDesc *boxes, int nbox, int val
 // ---------------------------------------------------------------------------
 // fix aboundary/meso (fix_aboundary_meso.cu:186-281, gpu_aboundary_v2 at end_of_step): for a
 // particle of the fix's group, project it half a kick and one drift ahead, sum a Gaussian
-// density of the wall particles among its list's core entries (the pairs within the cutoff at
-// the build), and where that density passes rho0/2 remove the parts of v and f pointing into
-// the wall.  FP32 as the reference, with its contractions spelled out.  The core entries are
-// recovered from the build positions (xh, packed exactly as the build packed them) with the
-// list build's FP32 test against the core cutoff.
+// density of the wall particles among its whole list row, and where that density passes rho0/2
+// remove the parts of v and f pointing into the wall.  The reference passes the row length as
+// dev_pair_count_core, which its list build's join (gpu_join_neigh_list,
+// neigh_build_meso.cu:188-204) has set to the core plus skin count: every entry of the row.
+// FP32 as the reference, with its contractions spelled out.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float3 packed_at_build(const BoxDesc &B, int j)
-{
-    int s = j, code = 13;
-    if (j >= B.nlocal) {
-        s = MDPD_IDX(B.gsrc[j - B.nlocal], B.nlocal);
-        code = B.gimg[j - B.nlocal];
-    }
-    return make_float3((float)(B.xh[0][s] + (code % 3 - 1) * B.prd[0] - B.cen[0]),
-                       (float)(B.xh[1][s] + ((code / 3) % 3 - 1) * B.prd[1] - B.cen[1]),
-                       (float)(B.xh[2][s] + (code / 9 - 1) * B.prd[2] - B.cen[2]));
-}
-
 // a.x*b.x + a.y*b.y + a.z*b.z as nvcc contracts it (the form of dist2)
 __device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz)
 {
@@ -278,8 +266,7 @@ __global__ void __launch_bounds__(kUnit) k_aboundary_meso(BoxDesc *__restrict__ 
         const float4 x0 = B.pos[i];
         const float3 vp = make_float3(__fmaf_rn(hs, f0.x, v0.x), __fmaf_rn(hs, f0.y, v0.y), __fmaf_rn(hs, f0.z, v0.z));
         const float3 c1 = make_float3(__fmaf_rn(dt, vp.x, x0.x), __fmaf_rn(dt, vp.y, x0.y), __fmaf_rn(dt, vp.z, x0.z));
-        const float3 bi = packed_at_build(B, i);
-        const float sig = B.ab_sigma, rc2 = B.rc2_core, nf = B.ab_nfactor;
+        const float sig = B.ab_sigma, nf = B.ab_nfactor;
         const float ex = __fdiv_rn(-0.5f, sig);
         float rho_w = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
         const int n = MDPD_IDX(B.count[i], B.n_col + 1);
@@ -287,8 +274,6 @@ __global__ void __launch_bounds__(kUnit) k_aboundary_meso(BoxDesc *__restrict__ 
             const int j = MDPD_IDX(B.table[list_addr(i, k, B.n_col)], n_all(B));
             const int mj = j < B.nlocal ? B.mask[c][j] : B.mask[c][MDPD_IDX(B.gsrc[j - B.nlocal], B.nlocal)];
             if (!(mj & B.ab_wall_bit)) continue;
-            const float3 bj = packed_at_build(B, j);
-            if (!(dist2(bi.x - bj.x, bi.y - bj.y, bi.z - bj.z) <= rc2)) continue;  // not a core entry
             const float4 c2 = B.pos[j];
             const float dx = c1.x - c2.x, dy = c1.y - c2.y, dz = c1.z - c2.z;
             const float rsq = dist2(dx, dy, dz);

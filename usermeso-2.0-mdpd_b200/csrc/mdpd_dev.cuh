@@ -111,8 +111,7 @@ struct BoxDesc {
     // plus the skin (rn2_list, squared, with a 1e-3 margin over the FP32 rounding of positions)
     float rn2_list;
     int list_reduce;      // set by the batch that steps the box
-    float rc2_core;       // (cutoff)^2: entries within it at the build are the list's core
-    // fix aboundary/meso: Gaussian wall density over the core entries' wall particles
+    // fix aboundary/meso: Gaussian wall density over the wall particles of the list row
     int ab_mobile_bit, ab_wall_bit;
     float ab_rho0, ab_sigma, ab_nfactor;
     // ---- rebuild scratch ----
