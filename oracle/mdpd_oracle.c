@@ -602,21 +602,30 @@ void orc_density(int nlocal, const float *pos4, const int32_t *count, const int3
                  int n_col, const int32_t *mask, int groupbit, double cut_rho,
                  const double *mass_type, double *rho)
 {
-    /* fix_aboundary_rho_meso.cu:88-90 (factor) and :119-165 (kernel), in FP64 */
+    /* fix_aboundary_rho_meso.cu:88-90 (factor) and :119-165 (kernel).  The reference works in
+     * FP32 here and so does this restatement, step for step: the coordinate differences, the
+     * squared distance (contracted as orc_dr2f), r = rsq * rsqrt(rsq), (h - r)^2; the weight
+     * (h - r)^2 * factor is formed in FP64 and rounded to FP32 (r32 wf), and the sum of
+     * m_i * wf is FP64.  The reference's rsqrt is the hardware's approximate FP32 reciprocal
+     * square root; 1 / sqrtf (correctly rounded) stands in for it, so single terms may differ
+     * in their last bits. */
     const double factor = 15.0 / (2.0 * M_PI * cut_rho * cut_rho * cut_rho * cut_rho * cut_rho);
+    const float h = (float)cut_rho;
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < nlocal; ++i) {
         if (!(mask[i] & groupbit)) continue; /* not written, as in the reference */
-        double xi = pos4[4 * i], yi = pos4[4 * i + 1], zi = pos4[4 * i + 2];
+        const float xi = pos4[4 * i], yi = pos4[4 * i + 1], zi = pos4[4 * i + 2];
         double mi = mass_type[type_of(pos4, i)];
         double r = 0.0;
         for (int k = 0; k < count[i]; ++k) {
             int j = table[(size_t)i * n_col + k];
-            double dx = xi - pos4[4 * j], dy = yi - pos4[4 * j + 1], dz = zi - pos4[4 * j + 2];
-            double rsq = dx * dx + dy * dy + dz * dz;
-            if (rsq < cut_rho * cut_rho && rsq >= 1e-20) {
-                double d = cut_rho - sqrt(rsq);
-                r += mi * d * d * factor;
+            const float dx = xi - pos4[4 * j], dy = yi - pos4[4 * j + 1], dz = zi - pos4[4 * j + 2];
+            const float rsq = orc_dr2f(dx, dy, dz);
+            if (rsq < h * h && rsq >= 1e-20) {
+                const float rr = rsq * (1.0f / sqrtf(rsq));
+                const float d = h - rr;
+                const float wf = (float)((double)(d * d) * factor);
+                r += mi * (double)wf;
             }
         }
         rho[i] = r;
@@ -686,14 +695,17 @@ void orc_force_mdpd(int nlocal, const float *pos4, const float *vel4, const doub
         double fx = 0, fy = 0, fz = 0, vr[6] = {0, 0, 0, 0, 0, 0}, en = 0;
         for (int k = 0; k < count[i]; ++k) {
             int j = table[(size_t)i * n_col + k];
-            double dx = xi - pos4[4 * j], dy = yi - pos4[4 * j + 1], dz = zi - pos4[4 * j + 2];
+            /* r64 dx = coord1.x - coord2.x: an FP32 difference widened to FP64 */
+            double dx = (float)(xi - pos4[4 * j]), dy = (float)(yi - pos4[4 * j + 1]),
+                   dz = (float)(zi - pos4[4 * j + 2]);
             double rsq = dx * dx + dy * dy + dz * dz;
             const orc_mdpd_coeff *c = coeff + ti * ntype + type_of(pos4, j);
             if (!(rsq < c->cut * c->cut && rsq >= 1e-20)) continue;
             double r = sqrt(rsq);
             if (r < 1e-10) continue;
             double rinv = 1.0 / r;
-            double dvx = vxi - vel4[4 * j], dvy = vyi - vel4[4 * j + 1], dvz = vzi - vel4[4 * j + 2];
+            double dvx = (float)(vxi - vel4[4 * j]), dvy = (float)(vyi - vel4[4 * j + 1]),
+                   dvz = (float)(vzi - vel4[4 * j + 2]);
             double dot = dx * dvx + dy * dvy + dz * dvz;
             double wc = 1.0 - r / c->cut;
             double wcr = 1.0 - r / c->cut_r;
@@ -750,14 +762,17 @@ void orc_force_dpd(int nlocal, const float *pos4, const float *vel4, const int32
         double fx = 0, fy = 0, fz = 0, vr[6] = {0, 0, 0, 0, 0, 0}, en = 0;
         for (int k = 0; k < count[i]; ++k) {
             int j = table[(size_t)i * n_col + k];
-            double dx = xi - pos4[4 * j], dy = yi - pos4[4 * j + 1], dz = zi - pos4[4 * j + 2];
+            /* r64 dx = coord1.x - coord2.x: an FP32 difference widened to FP64 */
+            double dx = (float)(xi - pos4[4 * j]), dy = (float)(yi - pos4[4 * j + 1]),
+                   dz = (float)(zi - pos4[4 * j + 2]);
             double rsq = dx * dx + dy * dy + dz * dz;
             const orc_dpd_coeff *c = coeff + ti * ntype + type_of(pos4, j);
             if (!(rsq < c->cutsq && rsq >= 1e-20)) continue;
             double rn = orc_gaussian_tea4(si, f2u(vel4[4 * j + 3]));
             double r = sqrt(rsq);
             double rinv = 1.0 / r;
-            double dvx = vxi - vel4[4 * j], dvy = vyi - vel4[4 * j + 1], dvz = vzi - vel4[4 * j + 2];
+            double dvx = (float)(vxi - vel4[4 * j]), dvy = (float)(vyi - vel4[4 * j + 1]),
+                   dvz = (float)(vzi - vel4[4 * j + 2]);
             double dot = dx * dvx + dy * dvy + dz * dvz;
             double wc = 1.0 - r * c->cutinv;
             double wr = c->expw == 1.0 ? wc : pow(wc, c->expw);

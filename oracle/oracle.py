@@ -137,6 +137,7 @@ def rebuild(x, typ, lo, hi, cutforce, skin, rho_est):
                        P(key, C.c_uint64), C.byref(nbits))
     perm = np.zeros(n, np.int32)
     L.orc_stable_sort_u64(n, P(key, C.c_uint64), P(perm, C.c_int32))
+    key_in = key.copy()  # reorder key of each particle, input (tag) order
     xs, ys, zs, key = xs[perm].copy(), ys[perm].copy(), zs[perm].copy(), key[perm]
     tags = (perm + 1).astype(np.int32)
     typ = np.ascontiguousarray(np.asarray(typ, np.int32)[perm])
@@ -161,7 +162,8 @@ def rebuild(x, typ, lo, hi, cutforce, skin, rho_est):
     ovf = L.orc_build_list(C.byref(b), n, n + ng, P(xa, C.c_double), P(ya, C.c_double), P(za, C.c_double),
                            P(pos4, C.c_float), P(cnt, C.c_int32), P(core, C.c_int32), P(table, C.c_int32))
     table = table.reshape(n, b.n_col)
-    return dict(box=b, perm=perm, tags=tags, x=np.stack([xs, ys, zs], 1), n_bulk=n_bulk, gsrc=gsrc, gimg=gimg,
+    return dict(box=b, perm=perm, tags=tags, key=key_in, x=np.stack([xs, ys, zs], 1), n_bulk=n_bulk, gsrc=gsrc,
+                gimg=gimg,
                 pos4=pos4, count=cnt, count_core=core, table=table, overflow=ovf, nbits=nbits.value)
 
 

@@ -10,8 +10,12 @@ energy tolerances are measured against.  No GPU.
   the virial, each halved per particle;
 - classic DPD: gpu_dpd (pair_dpd_meso.cu:91-205) with w_r = w_c^expw.
 
-xi is the pinned pairwise gaussian (test_oracle_pins).  Both sides compute in FP64 from the same
-FP32 inputs and differ only in summation order: agreement to 1e-12 of the summed magnitudes.
+xi is the pinned pairwise gaussian (test_oracle_pins).  The force passes form the coordinate and
+velocity differences in FP32 and everything after in FP64, as the reference does, on both sides:
+agreement to 1e-12 of the summed magnitudes.  The reference's density pass is FP32 throughout
+with the hardware rsqrt; the oracle follows its FP32 steps and this numpy restatement stays FP64,
+so the two agree to 2e-6 of rho (tests/test_oracle_ref_pin.py pins the oracle to the reference's
+own output at 1e-6 of the mean density).
 """
 import numpy as np
 
@@ -38,11 +42,11 @@ def setup(seed, ntype=2):
 
 
 def pair_geometry(pos4, vel4, I, J):
-    p = pos4.astype(np.float64)
-    v = vel4[:, :3].astype(np.float64)
-    d = p[I, :3] - p[J, :3]
+    # r64 dx = coord1.x - coord2.x with FP32 members: the difference is rounded to FP32
+    d = (pos4[I, :3] - pos4[J, :3]).astype(np.float64)
+    dv = (vel4[I, :3] - vel4[J, :3]).astype(np.float64)
     rsq = np.einsum("ij,ij->i", d, d)
-    dot = np.einsum("ij,ij->i", d, v[I] - v[J])
+    dot = np.einsum("ij,ij->i", d, dv)
     return d, rsq, dot
 
 
@@ -66,7 +70,7 @@ def test_density_matches_numpy():
     w = np.where(ok, (h - np.sqrt(rsq)) ** 2, 0.0) * mass_type[ptype[I]] * 15.0 / (2 * np.pi * h ** 5)
     want = sum_rows(n, I, w)
     want[mask[:n] & 1 == 0] = 0.0
-    assert np.all(np.abs(rho - want) <= 1e-12 * (np.abs(want) + 1))
+    assert np.all(np.abs(rho - want) <= 2e-6 * (np.abs(want) + 1))
     assert (want > 0).sum() > 0.8 * n
 
 
