@@ -4,9 +4,18 @@ pair-kernel HBM roofline on a 4M-particle box, served p50/p99 latency, the CPU b
 the end-to-end number through the C ABI.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --profile-box N [--equil E] [--steps S] [--shape D] [--rebuild]
 
 N > 1 runs under torchrun, one rank per GPU, each rank stepping its own 256-box set (weak
 scaling, no collective on the data path); rank 0 prints ONE JSON line.
+
+--profile-box N is the profiling leg (one GPU, for ncu launch lists and captures): one cubic
+mDPD box of N particles (rho 6.05, A -40, B 25, r_d 0.75, skin 0.3) stepped E times, then S steps
+in profile mode inside the NVTX range "prof" (integrate, rebuild, density and force as separate
+launches timed with CUDA events; `ncu --nvtx --nvtx-include "prof/"` selects them) and, with
+--rebuild, one forced full rebuild inside the range "rb".  --shape pins the density pass's
+neighbour gathers in flight (4, 6 or 8).  Prints one JSON line with the per-phase milliseconds
+and the graph step time.
 """
 import argparse
 import json
@@ -176,6 +185,33 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def profile_box(args):
+    import torch
+    import mdpd
+    n = args.profile_box
+    L = (n / RHO) ** (1 / 3)
+    b = mdpd.Batch([mdpd.box_spec(n, L, A=-40.0, B=25.0, seed=4242, init_seed=99)])
+    if args.shape:
+        b.set_shapes(args.shape)
+    b.setup()
+    b.step(args.equil)
+    r0 = b.rebuild_steps()
+    torch.cuda.nvtx.range_push("prof")
+    p = b.profile(args.steps)
+    torch.cuda.nvtx.range_pop()
+    out = {"particles": n, "shape": args.shape or "default", "profile_ms": p,
+           "rebuild_steps": b.rebuild_steps() - r0}
+    if args.rebuild:
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("rb")
+        b.setup()
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+    out["graph_ms_per_step"] = b.time(args.steps)
+    b.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -184,7 +220,13 @@ def main():
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--equil", type=int, default=300, help="untimed equilibration steps from the random start")
     ap.add_argument("--no-extras", action="store_true", help="skip plain/served/roofline/cpu legs")
+    ap.add_argument("--profile-box", type=int, default=0, help="profiling leg: one cubic box of this many particles")
+    ap.add_argument("--shape", type=int, default=0, help="profiling leg: pinned density shape (4, 6, 8)")
+    ap.add_argument("--rebuild", action="store_true", help="profiling leg: one forced rebuild in the range rb")
     args = ap.parse_args()
+    if args.profile_box:
+        profile_box(args)
+        return
     rank = int(os.environ.get("RANK", "0")); world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":

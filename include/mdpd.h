@@ -140,6 +140,9 @@ typedef struct mdpd_box_spec {
 
 int mdpd_batch_create(mdpd_batch_t **b, const mdpd_box_spec *specs, int32_t nbox, const mdpd_opts *opts);
 int mdpd_batch_setup(mdpd_batch_t *b);
+/* nsteps steps of every box; the last one also computes pair energy and virial, so the thermo
+ * read after the call (pressure, energy, virial, surface tension) is that step's, as the thermo
+ * line at the end of a LAMMPS run (Run::command, run.cpp:170-178) */
 int mdpd_batch_step(mdpd_batch_t *b, int64_t nsteps);
 int mdpd_batch_thermo(mdpd_batch_t *b, int32_t box, mdpd_thermo_t *out);
 /* every box's thermo in one pass (out[nbox], batch order; nbox must equal the batch's): the
@@ -164,6 +167,10 @@ int mdpd_batch_tune(mdpd_batch_t *b, int32_t *shape_density, int32_t *shape_forc
  * keeps nothing across runs (autotuner_meso.h:11-96). */
 int mdpd_batch_tune_cached(mdpd_batch_t *b, const char *path, int32_t *shape_density, int32_t *shape_force,
                            int32_t *cached);
+/* pin the pair-pass shapes (as mdpd_batch_tune reports them) without timing: one of the shapes
+ * the batch's pass family offers, else MDPD_ERR_ARG.  No reference counterpart: the reference's
+ * launch shapes come from its occupancy table (occupancy_meso.cu:8-50). */
+int mdpd_batch_set_shapes(mdpd_batch_t *b, int32_t shape_density, int32_t shape_force);
 /* last per-step device time in milliseconds measured with CUDA events over nsteps */
 int mdpd_batch_time(mdpd_batch_t *b, int64_t nsteps, double *ms_per_step);
 /* nsteps un-captured steps with CUDA events around each kernel group (same kernels as the

@@ -1060,7 +1060,9 @@ int orc_sim_run(orc_sim *s, int64_t nsteps)
             }
         }
         if (flag) err |= sim_rebuild(s);
-        sim_forces(s, 0);
+        /* energy and virial on the run's last step, from that step's own force call (a LAMMPS
+         * thermo step sets eflag/vflag on it; no extra force evaluation) */
+        sim_forces(s, it == nsteps - 1);
         /* final_integrate (fix_nve_meso.cu:157-178) */
         for (int i = 0; i < n; ++i) {
             if (!(s->mask[i] & s->p.nve_groupbit)) continue;
@@ -1096,12 +1098,16 @@ void orc_sim_get(const orc_sim *s, double *x, double *v, double *f, double *rho)
 int64_t orc_sim_step(const orc_sim *s) { return s->step; }
 int64_t orc_sim_nbuild(const orc_sim *s) { return s->nbuild; }
 
-void orc_sim_thermo(orc_sim *s, double out[8])
+void orc_sim_thermo(orc_sim *s, double out[14])
 {
     /* T: sum m v^2 / (3 N kB) over the nve group (compute_temp_meso.cu:58-101),
-     * virial trace, pair energy (forces recomputed with evflag), total momentum */
-    sim_forces(s, 1);
-    double ke = 0, vir = 0, pe = 0, px = 0, py = 0, pz = 0;
+     * virial trace, pair energy (from the last step's force call: setup and the last step of
+     * every run compute them), total momentum, and the pressure tensor times the volume,
+     * sum m v_a v_b + sum of the per-atom virials over all atoms (xx yy zz xy xz yz: the
+     * library's thermo ptensor times V).  Nothing is recomputed: a force evaluation here
+     * would replace the step's forces with ones from the full-step velocities and perturb the
+     * next step */
+    double ke = 0, vir = 0, pe = 0, px = 0, py = 0, pz = 0, pt[6] = {0, 0, 0, 0, 0, 0};
     int cnt = 0;
     for (int i = 0; i < s->n; ++i) {
         double m = s->p.mass_type[s->type[i] - 1];
@@ -1114,6 +1120,9 @@ void orc_sim_thermo(orc_sim *s, double out[8])
         px += m * s->vx[i];
         py += m * s->vy[i];
         pz += m * s->vz[i];
+        const double v[3] = {s->vx[i], s->vy[i], s->vz[i]};
+        const int ab[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+        for (int q = 0; q < 6; ++q) pt[q] += m * v[ab[q][0]] * v[ab[q][1]] + s->virial[6 * i + q];
     }
     out[0] = cnt > 1 ? ke / (3.0 * cnt - 3.0) : 0.0; /* dof = 3N - 3 (extra_dof) */
     out[1] = vir;
@@ -1123,6 +1132,7 @@ void orc_sim_thermo(orc_sim *s, double out[8])
     out[5] = pz;
     out[6] = (double)s->nbuild;
     out[7] = (double)s->step;
+    for (int q = 0; q < 6; ++q) out[8 + q] = pt[q];
 }
 
 /* correctly rounded fused multiply-add, for checks written in Python */

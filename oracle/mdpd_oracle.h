@@ -179,8 +179,9 @@ int orc_sim_run(orc_sim *s, int64_t nsteps);
 void orc_sim_get(const orc_sim *s, double *x, double *v, double *f, double *rho);
 int64_t orc_sim_step(const orc_sim *s);
 int64_t orc_sim_nbuild(const orc_sim *s);
-/* thermo: temperature (compute_temp_meso.cu:58-101), virial trace sum, PE, momentum */
-void orc_sim_thermo(orc_sim *s, double out[8]);
+/* thermo: temperature (compute_temp_meso.cu:58-101), virial trace sum, PE, momentum, build
+ * count, step, and the pressure tensor times the volume (xx yy zz xy xz yz) */
+void orc_sim_thermo(orc_sim *s, double out[14]);
 
 #ifdef __cplusplus
 }

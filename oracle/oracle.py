@@ -318,9 +318,13 @@ class Sim:
         return x, v, f, r
 
     def thermo(self):
-        o = np.zeros(8)
+        o = np.zeros(14)
         lib().orc_sim_thermo(self.h, P(o, C.c_double))
-        return dict(temp=o[0], virial=o[1], pe=o[2], momentum=o[3:6], nbuild=o[6], step=o[7])
+        vol = float(np.prod(np.array(self.p.hi[:]) - np.array(self.p.lo[:])))
+        ptensor = o[8:14] / vol
+        lx = self.p.hi[0] - self.p.lo[0]
+        return dict(temp=o[0], virial=o[1], pe=o[2], momentum=o[3:6], nbuild=o[6], step=o[7], ptensor=ptensor,
+                    surface_tension=0.5 * lx * (ptensor[0] - 0.5 * (ptensor[1] + ptensor[2])))
 
     def close(self):
         if self.h:

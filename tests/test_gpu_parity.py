@@ -4,8 +4,10 @@ Tolerances (stated per result):
   sort permutation, ghost images, pair sets, packed FP32 positions, RNG words: bit-exact
   FP64 gaussian (parity mode): bit-exact;  FP32 gaussian: |err| <= 3e-6 (absolute)
   density rho (FP32 pass with the hardware rsqrt, as the reference, vs FP64 oracle): <= 5e-6 relative
-  conservative forces at sigma = 0 (FP32 pass vs FP64 oracle): |df| <= 1e-5 * |F|_scale,
-  |F|_scale = sum over the particle's pairs of |F_ij| (the magnitude being summed)
+  conservative forces at sigma = 0 (FP32 pass vs FP64 oracle), per particle:
+  |dF_i| <= 1e-5 * max(|F_i|, F_rms), F_rms the RMS of |F_i| over the box (relative where the
+  net force is not tiny; 1e-5 of the typical force where the pair forces nearly cancel); the
+  per-particle |dF_i|/|F_i| percentiles are printed (pytest -s)
   full forces with the random term (exact RNG): same bound
   one velocity-Verlet step (FP64 x, v from the same FP32 forces): bit-exact
 """
@@ -179,19 +181,17 @@ def test_density_matches_oracle():
     assert np.max(np.abs(rho[:n] - ref) / ref) < 5e-6
 
 
-def force_scale(pos, cnt, rows, coeffs, rho, n):
-    # sum_j |F_ij| per particle (conservative part), the size of the terms the pass sums
-    s = np.zeros(n)
-    c = coeffs[(0, 0)]
-    for i in range(n):
-        js = rows[i, :cnt[i]]
-        d = pos[i, :3].astype(np.float64) - pos[js, :3].astype(np.float64)
-        r = np.sqrt((d * d).sum(1))
-        m = (r < c[0]) & (r > 1e-10)
-        wc = 1 - r[m] / c[0]
-        wr = np.maximum(1 - r[m] / c[1], 0)
-        s[i] = np.abs(c[2] * wc + c[3] * (rho[i] + rho[js[m]]) * wr).sum()
-    return s
+def assert_force_bar(f, ref, label, mask=None):
+    """|dF_i| <= 1e-5 * max(|F_i|, F_rms) for every particle; prints the relative-error percentiles"""
+    if mask is not None:
+        f, ref = f[mask], ref[mask]
+    mag = np.linalg.norm(ref, axis=1)
+    err = np.linalg.norm(f - ref, axis=1)
+    frms = np.sqrt(np.mean(mag ** 2))
+    rel = err / np.maximum(mag, 1e-30)
+    print(f"\n{label}: |dF_i|/|F_i| median {np.median(rel):.2e} p99.9 {np.quantile(rel, 0.999):.2e} "
+          f"max {rel.max():.2e}; max |dF_i|/F_rms {err.max() / frms:.2e}")
+    assert np.all(err <= 1e-5 * np.maximum(mag, frms)), (err / np.maximum(mag, frms)).max()
 
 
 @pytest.mark.parametrize("exact", [False, True])
@@ -204,9 +204,7 @@ def test_conservative_force_sigma0(exact):
     f = lam.field("force")[:, :3].astype(np.float64)
     coeffs = {(0, 0): (1.0, 0.75, -40.0, 25.0, 0.0, 0.0)}
     ref = oracle.force_mdpd(pos, vel, rho, cnt, rows, coeffs, 0.01)
-    scale = force_scale(pos, cnt, rows, coeffs, rho, n)
-    err = np.abs(f - ref).max(1)
-    assert np.all(err <= 1e-5 * scale + 1e-6), (err / scale).max()
+    assert_force_bar(f[:n], ref, f"sigma=0 forces ({'exact' if exact else 'fast'} rng)")
 
 
 def test_full_force_with_exact_rng():
@@ -219,9 +217,7 @@ def test_full_force_with_exact_rng():
     sigma = np.sqrt(2 * 1.0 * 4.5)
     coeffs = {(0, 0): (1.0, 0.75, -40.0, 25.0, 4.5, sigma)}
     ref = oracle.force_mdpd(pos, vel, rho, cnt, rows, coeffs, 0.01)
-    scale = force_scale(pos, cnt, rows, coeffs, rho, n) + np.abs(ref).max(1)
-    err = np.abs(f - ref).max(1)
-    assert np.all(err <= 1e-5 * scale + 1e-5), (err / scale).max()
+    assert_force_bar(f[:n], ref, "full forces (exact rng)")
 
 
 def test_velocity_verlet_step_bit_exact():
@@ -262,8 +258,7 @@ def test_dpd_pairs_signatures_and_forces():
     pos = lam.field("pos4")
     f = lam.field("force")[:, :3].astype(np.float64)
     reff = oracle.force_dpd(pos, vel, cnt, rows, {(0, 0): (1.0, 25.0, 4.5, 3.0, 1.0)}, 0.01)
-    scale = np.abs(reff).max(1) + 25.0
-    assert np.all(np.abs(f - reff).max(1) <= 1e-5 * scale)
+    assert_force_bar(f[:n], reff, "classic DPD forces")
 
 
 def test_list_overflow_reported_not_crashed():
@@ -323,26 +318,16 @@ run_style mvv/meso
     coeffs = {(0, 0): (1.0, 0.75, -40.0, 25.0, 0.0, 0.0), (0, 1): (1.0, 0.70, -30.0, 20.0, 0.0, 0.0),
               (1, 0): (1.0, 0.70, -30.0, 20.0, 0.0, 0.0), (1, 1): (0.9, 0.75, -50.0, 30.0, 0.0, 0.0)}
     ref = oracle.force_mdpd(pos, vel, rho, cnt, rows, coeffs, 0.01)
-    # |F| scale: the summed magnitudes of the conservative pair terms
-    typ = (pos[:, 3].view(np.int32) & 0xFF)
-    s = np.zeros(n)
-    for i in range(n):
-        js = rows[i, :cnt[i]]
-        d = pos[i, :3].astype(np.float64) - pos[js, :3].astype(np.float64)
-        r = np.sqrt((d * d).sum(1))
-        for jj, rr in zip(js, r):
-            c = coeffs[(int(typ[i]), int(typ[jj]))]
-            if 1e-10 < rr < c[0]:
-                s[i] += abs(c[2] * (1 - rr / c[0]) + c[3] * (rho[i] + rho[jj]) * max(1 - rr / c[1], 0))
-    err = np.abs(f - ref).max(1)
-    assert np.all(err <= 1e-5 * s + 1e-6), (err / (s + 1e-12)).max()
+    assert_force_bar(f[:n], ref, "two-type sigma=0 forces")
 
 
-@pytest.mark.parametrize("A", [float("inf"), -1e12])
+@pytest.mark.parametrize("A", [float("inf"), -1e12, -2e8])
 def test_nonfinite_or_out_of_range_force_reported(A):
-    # injected on the host through the coefficients: an infinite A gives non-finite forces, and
-    # A = -1e12 forces beyond the fixed-point sums' range (|F| < 1e9); both come back as
-    # MDPD_ERR_NAN from the call, the context stays usable
+    # injected on the host through the coefficients: an infinite A gives non-finite forces;
+    # A = -1e12 gives single pair terms beyond the fixed-point range; A = -2e8 gives pair terms
+    # of ~1e8, each inside the int64 range of 2^-32 units but ~25 of them add past 2^31, where a
+    # particle's sum would wrap -- the per-pair bound 2^31 / (n_col + 1) catches them.  All come
+    # back as MDPD_ERR_NAN from the call and the context stays usable
     lam = mdpd_box(A=A)
     with pytest.raises(mdpd.MdpdError) as e:
         lam.setup()

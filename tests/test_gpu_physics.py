@@ -1,10 +1,11 @@
 """Statistical checks of whole runs on the GPU against the reference's decks and the oracle.
 
-Tolerances: temperature within 1-2% of the thermostat value in long runs (fluctuation-
-averaged), density profiles within 2% in the bulk bins of the reference's own deck output,
-mean local density within 2% of the FP64 oracle engine from the same start, total momentum
-drift below 1e-6 per particle after 1,000 steps (pair forces are antisymmetric bit for bit;
-the drift is the FP32 rounding of each particle's force sum).
+Tolerances: temperature within 1% of the FP64 oracle engine run from the same start
+(fluctuation-averaged; the spec's bar) and within 1-2% of the thermostat value, density profiles
+within 2% in the bulk bins of the reference's own deck output, mean local density within 2% of
+the oracle engine from the same start, total momentum drift below 1e-6 per particle after 1,000
+steps (pair forces are antisymmetric bit for bit; the drift is the FP32 rounding of each
+particle's force sum).
 """
 import gzip
 import json
@@ -65,10 +66,11 @@ def test_mdpd_liquid_temperature_and_density():
     sim.setup()
     b.step(400); sim.run(400)
     tg, to, rg, ro = [], [], [], []
-    for _ in range(8):
+    for k in range(40):
         b.step(25); sim.run(25)
         tg.append(b.thermo(0).temp); to.append(sim.thermo()["temp"])
-        ro.append(sim.state()[3].mean())
+        if k % 5 == 4:
+            ro.append(sim.state()[3].mean())
     lam = mdpd.Lammps()  # GPU mean local density through the script path on the same start
     lam.commands(f"""
 units lj
@@ -90,6 +92,9 @@ run_style mvv/meso
     for _ in range(8):
         lam.run(25)
         rg.append(lam.field("rho")[:n].mean())
+    # T against the oracle engine within the spec's 1%; each within 2% of kT (the mDPD liquid at
+    # dt = 0.01 runs slightly hot in both)
+    assert abs(np.mean(tg) - np.mean(to)) < 0.01 * np.mean(to), (np.mean(tg), np.mean(to))
     assert abs(np.mean(tg) - 1.0) < 0.02 and abs(np.mean(to) - 1.0) < 0.02
     assert abs(np.mean(rg) - np.mean(ro)) / np.mean(ro) < 0.02, (np.mean(rg), np.mean(ro))
 
@@ -154,7 +159,10 @@ fix dn group_fluid1 density/meso along y nbin 10 every 99999 window 99998 output
 
 
 def test_gpu_temperature_agrees_with_oracle_engine():
-    # same initial state through the GPU path and the FP64 oracle engine: ensemble averages agree
+    # config 1 (classic DPD: 10^3 box, rho 3, a 25, gamma 4.5, sigma 3, dt 0.01): the same start
+    # through the GPU path and the FP64 oracle engine; after 500 relaxation steps, 200 samples 10
+    # steps apart.  The two mean temperatures agree within 1% (the spec's bar) and both sit within
+    # 1% of kT.
     rng = np.random.default_rng(5)
     n, L = 3000, 10.0
     x = rng.uniform(0, L, (n, 3))
@@ -164,8 +172,13 @@ def test_gpu_temperature_agrees_with_oracle_engine():
     b.setup()
     sim = oracle.Sim(x, v, (0, 0, 0), (L, L, L), style=1, a0=25.0, gamma=4.5, sigma=3.0, seed=99, rho_est=0.0)
     sim.setup()
+    b.step(500); sim.run(500)
     tg, to = [], []
-    for _ in range(10):
-        b.step(30); sim.run(30)
+    for _ in range(200):
+        b.step(10); sim.run(10)
         tg.append(b.thermo(0).temp); to.append(sim.thermo()["temp"])
-    assert abs(np.mean(tg) - np.mean(to)) < 0.03
+    sim.close()
+    b.close()
+    tg, to = np.mean(tg), np.mean(to)
+    assert abs(tg - to) < 0.01 * to, (tg, to)
+    assert abs(tg - 1.0) < 0.01 and abs(to - 1.0) < 0.01, (tg, to)

@@ -10,7 +10,8 @@ into the empty core (seen with a 1.3-thick layer).
 
 Checked after 3,000 steps: no fluid particle newly inside a cylinder's wall-free core (beyond
 the wall layer) once the start-up transient is over, the fluid flowing along the body force with
-its mean x velocity growing, the fluid temperature within 5% of kT, and a clean device status."""
+its mean x velocity growing, the fluid temperature (averaged over the last 2,000 steps) within 1% of
+kT, and a clean device status."""
 import numpy as np
 import pytest
 
@@ -98,14 +99,18 @@ run_style mvv/meso
     x1, v1, _, _ = lam.state()
     vx1 = v1[:nf, 0].mean()
     core1 = int(np.sum(margin(np.mod(x1[:nf], (LX, LY, LZ))) <= -WALL))
-    lam.run(2000)
+    temps = []
+    for _ in range(20):  # the fluid's temperature over the last 2,000 steps
+        lam.run(100)
+        temps.append(lam.thermo().temp_group)
     x2, v2, tag, typ = lam.state()
     t = lam.thermo()
     lam.close()
     assert t.status == 0
     vx2 = v2[:nf, 0].mean()
     assert 0 < vx1 < vx2, (vx1, vx2)
-    assert abs(t.temp_group - 1.0) < 0.05, t.temp_group
+    print(f"\npore flow: fluid T over the last 2,000 steps {np.mean(temps):.4f} (samples {min(temps):.4f}..{max(temps):.4f})")
+    assert abs(np.mean(temps) - 1.0) < 0.01, temps
     # fluid in a cylinder's wall-free core (beyond the wall layer): at most the few that the
     # random start's overlaps shot through it in the first steps, and in steady flow no more than
     # rare events (1e-5 of the fluid over 2,000 steps; a 1.3-thick layer leaked ~1.5e-4)

@@ -6,11 +6,13 @@ the library's script surface (read_data of the same particles, the same styles a
 coefficients, reset_timestep to the same step) and its setup pass -- rebuild, density, forces --
 is compared with them:
 
-  sort permutation (tags in internal order), packed FP32 positions, TEA signatures   bit-exact
+  sort permutation (tags in internal order), packed FP32 positions (x, y, z and the type byte
+  of w; the library packs its own wall flags above it), TEA signatures                bit-exact
   neighbour rows of every particle as (count, order-free hash of the neighbour tags): the
   reference's full rows on boxes that keep the full list, its rows reduced by the pair-once
   rule (owned entries and those within r_d + skin + 1e-3) otherwise                   bit-exact
-  rho: FP32 on both sides with the hardware rsqrt                 |d rho_i| <= 1e-6 * mean rho
+  rho: the same FP32 terms (hardware rsqrt); summed in FP32 here, in FP64 by the reference
+                                                                  |d rho_i| <= 2e-6 * mean rho
   force (FP32 pair arithmetic, exact FP64 gaussian, against the reference's FP64 arithmetic on
   the same FP32 inputs and its own rho): |dF_i| <= 1e-5 * max(|F_i|, F_rms), F_rms the RMS of
   |F_i| over the box; the per-particle relative error is printed (pytest -s)
@@ -121,7 +123,9 @@ def test_packed_positions_and_signatures_bit_exact(setup_case):
         pytest.skip("large case: packed bits not stored")
     n = c["n"]
     order = np.argsort(lam.field("tag"))
-    assert np.array_equal(lam.field("pos4")[:n].view(np.uint32)[order], F["pos_bits"])
+    bits = lam.field("pos4")[:n].view(np.uint32)[order].copy()
+    bits[:, 3] &= 0xFF  # type - 1; bits 8 and up hold the library's mobile/wall flags
+    assert np.array_equal(bits, F["pos_bits"])
     assert np.array_equal(lam.field("vel4")[:n, 3].view(np.uint32)[order], F["sig"])
 
 
@@ -132,7 +136,7 @@ def test_density_matches_reference(setup_case):
     err = np.abs(rho - F["rho"])
     print(f"\n{c['name']}: rho max |d| / mean = {err.max() / F['rho'].mean():.2e}, "
           f"max rel = {(err / np.maximum(F['rho'], 1e-30)).max():.2e}")
-    assert err.max() <= 1e-6 * F["rho"].mean()
+    assert err.max() <= 2e-6 * F["rho"].mean()
 
 
 def test_force_matches_reference(setup_case):

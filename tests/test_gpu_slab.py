@@ -7,11 +7,16 @@ dt = 0.01), within 1% at full size (108,900 particles, 18,000 sampled steps), an
 mean T within 0.5% or 3 combined standard errors of each other;
 gamma > 0 and the two RNG modes agree within 2% of gamma or 3 combined standard errors (block
 averages), whichever is larger; liquid plateau density within 2%.
+
+A slab small enough for the FP64 oracle engine (6,050 particles) runs from the same start through
+both: T within 1% of the oracle's, the liquid plateau density within 2%, the surface tension
+within 2% of the oracle's or 3 combined standard errors, whichever is larger.
 """
 import numpy as np
 import pytest
 
 import mdpd
+import oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -125,3 +130,41 @@ def test_config2_slab_full_size():
     top_f = np.sort(pf)[-14:].mean(); top_e = np.sort(pe)[-14:].mean()
     assert abs(top_f - top_e) / top_e < 0.02, (top_f, top_e)
     assert 5.5 < top_f < 7.5
+
+
+def test_small_slab_against_oracle_engine():
+    # box [-12,12] x [-5,5]^2, liquid |x| < 5 at rho 6.05 (6,050 particles), A -40, B 25, r_d 0.75,
+    # gamma 4.5, kT 1, dt 0.01; the same positions and velocities through the GPU path and the
+    # FP64 oracle engine: 1,000 relaxation steps, then 4,000 steps sampled every 20
+    rng = np.random.default_rng(77)
+    lo, L = np.array([-12.0, -5.0, -5.0]), np.array([24.0, 10.0, 10.0])
+    n = int(round(6.05 * 10.0 * 10.0 * 10.0))
+    x = np.column_stack([rng.uniform(-5, 5, n), rng.uniform(-5, 5, n), rng.uniform(-5, 5, n)])
+    v = rng.normal(0, 1, (n, 3)); v -= v.mean(0)
+    b = mdpd.Batch([mdpd.box_spec(n, L, lo=lo, x=x, v=v, seed=31337)])
+    b.setup()
+    sim = oracle.Sim(x, v, tuple(lo), tuple(lo + L), seed=31337)
+    sim.setup()
+    b.step(1000); sim.run(1000)
+    tg, to, gg, go = [], [], [], []
+    hg, ho = np.zeros(24), np.zeros(24)
+    for _ in range(200):
+        b.step(20); sim.run(20)
+        t = b.thermo(0); o = sim.thermo()
+        tg.append(t.temp); to.append(o["temp"]); gg.append(t.surface_tension); go.append(o["surface_tension"])
+        xg, _ = b.state(0); xo = sim.state()[0]
+        hg += np.histogram(np.mod(xg[:, 0] + 12.0, 24.0), bins=24, range=(0, 24))[0]
+        ho += np.histogram(np.mod(xo[:, 0] + 12.0, 24.0), bins=24, range=(0, 24))[0]
+    sim.close()
+    b.close()
+    tg, to, gg, go = map(np.array, (tg, to, gg, go))
+    assert abs(tg.mean() - to.mean()) < 0.01 * to.mean(), (tg.mean(), to.mean())
+    # the slab drifts as a whole along x: the plateau is the densest 6 one-wide bins
+    plat_g = np.sort(hg)[-6:].mean() / (200 * 100.0)
+    plat_o = np.sort(ho)[-6:].mean() / (200 * 100.0)
+    assert abs(plat_g - plat_o) < 0.02 * plat_o, (plat_g, plat_o)
+    assert gg.mean() > 0 and go.mean() > 0
+    tol = max(0.02 * abs(go.mean()), 3 * np.hypot(block_se(gg), block_se(go)))
+    assert abs(gg.mean() - go.mean()) < tol, (gg.mean(), go.mean(), tol)
+    print(f"\nsmall slab: T {tg.mean():.4f} vs oracle {to.mean():.4f}; plateau {plat_g:.3f} vs {plat_o:.3f}; "
+          f"gamma {gg.mean():.3f} +- {block_se(gg):.3f} vs {go.mean():.3f} +- {block_se(go):.3f}")

@@ -493,7 +493,7 @@ int mdpd_batch_step(mdpd_batch_t *b, int64_t nsteps)
 {
     if (!b || nsteps < 0) return MDPD_ERR_ARG;
     return guard(b->err, [&] {
-        b->batch->run(nsteps, true);
+        b->batch->run(nsteps, true, true);
         std::string msg;
         if (int st = b->batch->status(msg)) throw ScriptError(st & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, msg);
     });
@@ -693,6 +693,22 @@ int mdpd_batch_tune_cached(mdpd_batch_t *b, const char *path, int32_t *shape_den
         if (cached) *cached = hit ? 1 : 0;
         std::string msg;
         if (int st = b->batch->status(msg)) throw ScriptError(st & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, msg);
+    });
+}
+
+int mdpd_batch_set_shapes(mdpd_batch_t *b, int32_t shape_density, int32_t shape_force)
+{
+    if (!b) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        for (const StepConfig &c : tune_candidates(b->batch->cfg)) {
+            const TunePick q = pick_of(c, 0.0);
+            if (q.density == shape_density && q.force == shape_force) {
+                b->batch->reconfigure(c);
+                return;
+            }
+        }
+        throw std::runtime_error("ARG: shapes (" + std::to_string(shape_density) + ", " + std::to_string(shape_force) +
+                                 ") are not offered for this batch's pass family");
     });
 }
 

@@ -281,6 +281,7 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     B.nrow = ceil_to(n, 32);
     B.ghost_cap = (int)std::min<long long>(ghost_estimate(s, g, n), 8LL * n + 4096);
     B.n_col = g.n_col;
+    B.fix_pair_max = (float)(2147483648.0 / (double)(g.n_col + 1));
     B.every = std::max(1, s.every);
     B.delay = s.delay;
     B.check = s.check;
@@ -317,7 +318,7 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     B.nve_bit = s.nve_bit;
     B.rho_bit = s.rho_bit;
     B.cut_rho = (float)s.cut_rho;
-    B.rho_factor = (float)(15.0 / (2.0 * M_PI * std::pow(s.cut_rho, 5.0)));
+    B.rho_factor = 15.0 / (2.0 * M_PI * s.cut_rho * s.cut_rho * s.cut_rho * s.cut_rho * s.cut_rho);
     B.body_bit = s.body_bit;
     for (int d = 0; d < 3; ++d) B.body[d] = s.body[d];
     B.arb_bc = s.arb_bc;
@@ -649,10 +650,11 @@ void Batch::reconfigure(const StepConfig &c)
     capture(1);
 }
 
-void Batch::run(long long nsteps, bool sync)
+void Batch::run(long long nsteps, bool sync, bool ev_last)
 {
     Range r("mdpd::run");
-    for (long long k = 0; k < nsteps; ++k) check_cuda(cudaGraphLaunch(graph_[0], stream_), "graph launch");
+    for (long long k = 0; k < nsteps; ++k)
+        check_cuda(cudaGraphLaunch(graph_[ev_last && k == nsteps - 1 ? 1 : 0], stream_), "graph launch");
     if (sync) check_cuda(cudaStreamSynchronize(stream_), "run");
 }
 

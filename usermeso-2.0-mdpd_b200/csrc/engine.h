@@ -120,7 +120,9 @@ public:
     // passes rerun for all boxes, which reproduces the same forces for the others
     void setup_boxes(const std::vector<int> &which);
     void reconfigure(const StepConfig &c);  // new pair-pass shapes: recapture the step graphs
-    void run(long long nsteps, bool sync = true);  // nsteps graph replays
+    // nsteps graph replays; with ev_last the last one also computes energy and virial (the
+    // step a thermo line reports, as at the end of a LAMMPS run)
+    void run(long long nsteps, bool sync = true, bool ev_last = false);
     void step_ev();                        // one step with energy/virial (thermo step)
     // nsteps un-captured steps with CUDA events around each kernel group; per-step averages
     // in ms: [integrate, rebuild (all steps), density, force], plus steps that rebuilt

@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(kUnit *TPP, 16 / TPP) k_density(const BoxDesc 
 #pragma unroll
         for (int o = TPP / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (in_group && t == 0) {
-            const float r = (float)(B.mass[ptype(B.pos[i])] * (double)B.rho_factor) * acc;
+            const float r = (float)(B.mass[ptype(B.pos[i])] * B.rho_factor) * acc;
             B.rho[i] = r;
             if (i >= B.st->n_bulk) {
                 const int g1 = min(B.gfirst[i + 1], B.ghost_cap);

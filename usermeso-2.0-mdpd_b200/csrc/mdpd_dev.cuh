@@ -15,6 +15,7 @@ constexpr int kUnit = 128;          // particles per work unit (multiple of 32)
 constexpr int kClassMax = 512;      // largest bucket the in-warp bucket sort accepts
 constexpr int kWarpsPerBlock = 8;
 
+
 // error bits reported per box (status word), mirrored by MDPD_ERR_* in include/mdpd.h
 enum : int {
     kErrListOverflow = 1,   // a particle has more than n_col neighbours
@@ -80,7 +81,8 @@ struct BoxDesc {
     uint32_t seed;
     int nve_bit;
     int rho_bit;
-    float cut_rho, rho_factor;   // 15/(2 pi cut_rho^5)
+    float cut_rho;
+    double rho_factor;    // 15/(2 pi cut_rho^5), FP64 as the reference (fix_aboundary_rho_meso.cu:90)
     int body_bit;
     double body[3];       // fix addforce/meso: added in FP64 in both half-kicks (f holds the pair force)
     int arb_bc, mobile_bit, wall_bit;   // wall coupling (pair_style mdpd/meso ... fluid wall)
@@ -105,6 +107,11 @@ struct BoxDesc {
     int *count2, *table2;
     int n_col2;
     unsigned long long *facc;  // 3 x nlocal fixed-point force sums (2^-32 units), SoA
+    // largest |pair force component| the fixed-point sums accept: 2^31 / (n_col + 1).  A
+    // particle's sum has one term per full-list neighbour, at most n_col of them (a longer row
+    // is a list overflow), so terms below this bound add to less than 2^31 and the int64 sum in
+    // 2^-32 units cannot wrap; a larger term sets the non-finite status
+    float fix_pair_max;
     float rc2_force;      // largest force cutoff squared
     // pair-once boxes without walls keep, of the pairs within the list cutoff, only those the
     // passes can use before the next build: the owned ones and those within the density cutoff

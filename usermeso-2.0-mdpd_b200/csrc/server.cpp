@@ -194,7 +194,7 @@ void mdpd_server_s::loop()
         k = std::max<int64_t>(k, 1);
         Range chunk_range("mdpd::server_chunk");
         cudaEventRecord(e0, batch->stream());
-        batch->run(k, false);
+        batch->run(k, false, true);  // a retiring job's thermo reports its last step's energy and virial
         cudaEventRecord(e1, batch->stream());
         cudaEventSynchronize(e1);
         float ms = 0;

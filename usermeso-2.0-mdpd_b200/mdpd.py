@@ -92,6 +92,7 @@ def lib():
             "mdpd_batch_get_state": ([vp, i32, dp, dp, i64], C.c_int),
             "mdpd_batch_tune": ([vp, i32p, i32p], C.c_int),
             "mdpd_batch_tune_cached": ([vp, cp, i32p, i32p, i32p], C.c_int),
+            "mdpd_batch_set_shapes": ([vp, i32, i32], C.c_int),
             "mdpd_batch_time": ([vp, i64, dp], C.c_int),
             "mdpd_batch_profile": ([vp, i64, dp], C.c_int),
             "mdpd_batch_rebuild_steps": ([vp, C.POINTER(i64)], C.c_int),
@@ -349,6 +350,10 @@ class Batch:
         hit = C.c_int32()
         self._check(lib().mdpd_batch_tune_cached(self.h, os.fsencode(cache), C.byref(a), C.byref(b), C.byref(hit)))
         return a.value, b.value, bool(hit.value)
+
+    def set_shapes(self, density, force=32):
+        """pin the pair-pass shapes (the values tune() reports) without timing"""
+        self._check(lib().mdpd_batch_set_shapes(self.h, int(density), int(force)))
 
     def thermo(self, box):
         t = Thermo()
