@@ -369,8 +369,9 @@ int mdpd_gaussian(const uint32_t *si, const uint32_t *sj, double *exact, float *
 
 namespace mdpd {
 
-// synthetic box of a mdpd_box_spec: the physics and, if x is NULL, a seeded uniform fill
-void spec_from_box(const mdpd_box_spec &bs, Spec &s, Particles &p)
+// synthetic box of a mdpd_box_spec: the physics and, if x is NULL, the seeded device fill (uniform
+// positions in the fill region, Maxwell velocities at kT with zero net momentum)
+void spec_from_box(const mdpd_box_spec &bs, Spec &s, Fill &fill)
 {
     if (bs.n <= 0) throw std::runtime_error("ARG: box spec with n <= 0");
     s = Spec();
@@ -398,36 +399,13 @@ void spec_from_box(const mdpd_box_spec &bs, Spec &s, Particles &p)
     q.expw = 1.0;
     if (q.cut < q.cut_r) throw std::runtime_error("PARSE: cutA should be larger than cutB.");
     s.pair[0][0] = q;
-    const int n = bs.n;
-    p = Particles();
-    if (bs.x) return;  // the caller's arrays are used in place
-    p.x.resize(3 * (size_t)n);
-    p.v.resize(3 * (size_t)n);
-    p.tag.resize(n);
-    p.type.assign(n, 1);
-    p.mask.assign(n, 1);
-    for (int i = 0; i < n; ++i) p.tag[i] = i + 1;
-    std::mt19937_64 rng(bs.init_seed);
-    std::uniform_real_distribution<double> u(0.0, 1.0);
-    std::normal_distribution<double> g(0.0, 1.0);
-    double flo[3], fhi[3];
     for (int d = 0; d < 3; ++d) {
         const bool sub = bs.fill_hi[d] > bs.fill_lo[d];
-        flo[d] = sub ? std::max(bs.fill_lo[d], bs.lo[d]) : bs.lo[d];
-        fhi[d] = sub ? std::min(bs.fill_hi[d], bs.hi[d]) : bs.hi[d];
+        fill.lo[d] = sub ? std::max(bs.fill_lo[d], bs.lo[d]) : bs.lo[d];
+        fill.hi[d] = sub ? std::min(bs.fill_hi[d], bs.hi[d]) : bs.hi[d];
     }
-    const double sv = std::sqrt(bs.kT / s.mass[0]);
-    double mom[3] = {0, 0, 0};
-    for (int i = 0; i < n; ++i)
-        for (int d = 0; d < 3; ++d) {
-            double x = flo[d] + u(rng) * (fhi[d] - flo[d]);
-            if (x >= bs.hi[d]) x = bs.lo[d];
-            p.x[3 * i + d] = x;
-            p.v[3 * i + d] = sv * g(rng);
-            mom[d] += p.v[3 * i + d];
-        }
-    for (int i = 0; i < n; ++i)
-        for (int d = 0; d < 3; ++d) p.v[3 * i + d] -= mom[d] / n;
+    fill.seed = bs.init_seed;
+    fill.vscale = std::sqrt(bs.kT / s.mass[0]);
 }
 
 }  // namespace mdpd
@@ -453,13 +431,13 @@ int mdpd_batch_create(mdpd_batch_t **out, const mdpd_box_spec *specs, int32_t nb
                 if ((specs[k].exact_rng != 0) != (cfg.exact_rng != 0))
                     throw std::runtime_error("ARG: a batch holds boxes of one RNG mode (exact_rng)");
                 Spec s;
-                Particles p;
-                spec_from_box(specs[k], s, p);
+                Fill fill;
+                spec_from_box(specs[k], s, fill);
                 if (specs[k].x)  // the caller's arrays go to the device directly, the copies queued
                     b->boxes.emplace_back(
                         new Box(s, specs[k].n, specs[k].x, specs[k].v, nullptr, nullptr, nullptr, cfg.sms, false));
                 else
-                    b->boxes.emplace_back(new Box(s, p, cfg.sms));
+                    b->boxes.emplace_back(new Box(s, specs[k].n, fill, cfg.sms, false));
                 raw.push_back(b->boxes.back().get());
             }
         } catch (...) {

@@ -236,8 +236,21 @@ Box::Box(const Spec &s, int n_, const double *x, const double *v, const int32_t 
     }
 }
 
+Box::Box(const Spec &s, int n_, const Fill &fill, int sms, bool wait) : spec(s)
+{
+    Range r("mdpd::box_create");
+    (void)sms;
+    n = n_;
+    try {
+        init(s, nullptr, nullptr, nullptr, nullptr, nullptr, wait, &fill);
+    } catch (...) {
+        release();
+        throw;
+    }
+}
+
 void Box::init(const Spec &s, const double *x, const double *v, const int32_t *tag, const int32_t *type,
-               const int32_t *mask, bool wait)
+               const int32_t *mask, bool wait, const Fill *fill)
 {
     if (n <= 0) throw std::runtime_error("ARG: box has no particles");
     if (s.ntype < 1 || s.ntype > kMaxTypes) throw std::runtime_error("ARG: 1..8 atom types supported");
@@ -368,16 +381,24 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
         // the cached ranks outlive the queued copy
         check_cuda(cudaMemcpyAsync(B.bin_rank, rank.data(), sizeof(int) * nbin, cudaMemcpyHostToDevice, 0), "upload");
     }
-    // initial state into buffer 0: the caller's AoS x and v go to the list table's space (unused
-    // until the first build, which writes every entry it later reads), a kernel splits them
-    // into x, xh and v components and fills tags/types/masks that were not given
+    // initial state into buffer 0: the caller's AoS x and v (or a device fill of them) go to the
+    // list table's space (unused until the first build, which writes every entry it later
+    // reads), a kernel splits them into x, xh and v components and fills tags/types/masks that
+    // were not given
     {
-        if (!x) throw std::runtime_error("ARG: no positions");
+        if (!x && !fill) throw std::runtime_error("ARG: no positions");
         const size_t need = 6 * sizeof(double) * (size_t)n;
         if ((size_t)B.nrow * B.n_col * sizeof(int) < need) throw std::runtime_error("ARG: list table too small to stage");
         double *sx = reinterpret_cast<double *>(B.table), *sv = sx + 3 * (size_t)n;
-        check_cuda(cudaMemcpyAsync(sx, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, 0), "upload");
-        if (v) check_cuda(cudaMemcpyAsync(sv, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, 0), "upload");
+        if (fill) {
+            // the thermo partials (zeroed with the arena, rewritten by every thermo pass) hold
+            // the fill's momentum sum
+            launch_fill(0, *fill, s.lo, s.hi, n, sx, sv, reinterpret_cast<unsigned long long *>(B.partial));
+            v = sv;  // non-null: the split kernel takes the filled velocities
+        } else {
+            check_cuda(cudaMemcpyAsync(sx, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, 0), "upload");
+            if (v) check_cuda(cudaMemcpyAsync(sv, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, 0), "upload");
+        }
         if (tag) check_cuda(cudaMemcpyAsync(B.tag[0], tag, sizeof(int) * n, cudaMemcpyHostToDevice, 0), "upload");
         if (type) check_cuda(cudaMemcpyAsync(B.type[0], type, sizeof(int) * n, cudaMemcpyHostToDevice, 0), "upload");
         if (mask) check_cuda(cudaMemcpyAsync(B.mask[0], mask, sizeof(int) * n, cudaMemcpyHostToDevice, 0), "upload");
@@ -520,11 +541,13 @@ Batch::~Batch()
     if (stream_) cudaStreamDestroy(stream_);
 }
 
-void Batch::build_units()
+// units of the boxes `which` (indices into the batch); device arrays appended to allocs
+static BatchUnits make_units(const std::vector<Box *> &boxes, const std::vector<int> &which, int nbox,
+                             std::vector<Unit *> &allocs)
 {
     std::vector<Unit> loc, all, cls, bins, scls, sgh, sbin;
-    for (int b = 0; b < (int)boxes_.size(); ++b) {
-        const BoxDesc &B = boxes_[b]->desc;
+    for (int b : which) {
+        const BoxDesc &B = boxes[b]->desc;
         auto chunk = [&](std::vector<Unit> &v, int n, int step) {
             for (int s = 0; s < n; s += step) v.push_back({b, s, std::min(n, s + step)});
         };
@@ -540,17 +563,26 @@ void Batch::build_units()
         Unit *d = nullptr;
         check_cuda(cudaMalloc(&d, sizeof(Unit) * std::max<size_t>(v.size(), 1)), "units");
         check_cuda(cudaMemcpy(d, v.data(), sizeof(Unit) * v.size(), cudaMemcpyHostToDevice), "units");
-        unit_allocs_.push_back(d);
+        allocs.push_back(d);
         return UnitList{d, (int)v.size()};
     };
-    units.local = up(loc);
-    units.all = up(all);
-    units.cls = up(cls);
-    units.bins = up(bins);
-    units.scan_cls = up(scls);
-    units.scan_ghost = up(sgh);
-    units.scan_bin = up(sbin);
-    units.nbox = (int)boxes_.size();
+    BatchUnits u;
+    u.local = up(loc);
+    u.all = up(all);
+    u.cls = up(cls);
+    u.bins = up(bins);
+    u.scan_cls = up(scls);
+    u.scan_ghost = up(sgh);
+    u.scan_bin = up(sbin);
+    u.nbox = nbox;  // box-indexed kernels (scan tops, build counters) see every box of the batch
+    return u;
+}
+
+void Batch::build_units()
+{
+    std::vector<int> every(boxes_.size());
+    for (size_t b = 0; b < boxes_.size(); ++b) every[b] = (int)b;
+    units = make_units(boxes_, every, (int)boxes_.size(), unit_allocs_);
 }
 
 void Batch::capture(int ev)
@@ -624,13 +656,17 @@ void Batch::setup_boxes(const std::vector<int> &which)
     check_cuda(cudaMemcpyAsync(d, which.data(), sizeof(int) * which.size(), cudaMemcpyHostToDevice, stream_),
                "setup boxes");
     k_set_rebuild<<<1, 256, 0, stream_>>>(d_boxes, d, (int)which.size(), units.nbox);
-    launch_rebuild(stream_, d_boxes, units, cfg, d_done);
-    if (cfg.style == 0) launch_density(stream_, d_boxes, units, cfg);
-    launch_force(stream_, d_boxes, units, cfg, 1, 0);
+    // the passes visit the new boxes only (the others keep their state and forces)
+    std::vector<Unit *> allocs;
+    const BatchUnits su = make_units(boxes_, which, units.nbox, allocs);
+    launch_rebuild(stream_, d_boxes, su, cfg, d_done);
+    if (cfg.style == 0) launch_density(stream_, d_boxes, su, cfg);
+    launch_force(stream_, d_boxes, su, cfg, 1, 0);
     launch_force_rebuild_flag(stream_, d_boxes, units.nbox, 0);
     check_cuda(cudaFreeAsync(d, stream_), "setup boxes");
     check_cuda(cudaGetLastError(), "setup launch");
     check_cuda(cudaStreamSynchronize(stream_), "setup");
+    for (Unit *a : allocs) cudaFree(a);
 }
 
 void Batch::reconfigure(const StepConfig &c)

@@ -62,9 +62,19 @@ struct Thermo {
     int status = 0;
 };
 
+// a box filled on the device: positions uniform in [lo, hi) (a position that reaches the box's
+// hi folds to its lo), velocities Maxwell with standard deviation vscale per component and zero
+// net momentum, both from a counter-based hash of (seed, particle, component)
+struct Fill {
+    double lo[3], hi[3];
+    uint64_t seed;
+    double vscale;
+};
+
 class Box {
 public:
     Box(const Spec &spec, const Particles &p, int sms);
+    Box(const Spec &spec, int n, const Fill &fill, int sms, bool wait = true);
     // from caller arrays (AoS x[3n], v[3n]; v null: at rest; tag/type/mask null: tags 1..n,
     // type 1, mask 1), copied straight to the device without host staging. wait = false leaves
     // the copies queued on the legacy default stream: the caller synchronises it before it
@@ -103,7 +113,7 @@ private:
     void layout(const Spec &s, int na);
     void release() noexcept;  // returns the arena to the pool
     void init(const Spec &s, const double *x, const double *v, const int32_t *tag, const int32_t *type,
-              const int32_t *mask, bool wait = true);
+              const int32_t *mask, bool wait = true, const Fill *fill = nullptr);
     template <class T> T *alloc(size_t count);
 };
 
@@ -163,6 +173,9 @@ struct Range {
 std::string status_text(int bits);  // names of the set bits of a box status word
 std::string cuda_err(cudaError_t e);
 void check_cuda(cudaError_t e, const char *what);
+// AoS x[3n], v[3n] of a Fill on the device (stream s); mom: 3 zeroed words of device scratch
+void launch_fill(cudaStream_t s, const Fill &f, const double box_lo[3], const double box_hi[3], int n, double *xa,
+                 double *va, unsigned long long *mom);
 int sm_count();
 
 }  // namespace mdpd

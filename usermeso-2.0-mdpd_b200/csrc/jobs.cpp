@@ -24,7 +24,7 @@
 
 namespace mdpd {
 
-void spec_from_box(const mdpd_box_spec &bs, Spec &s, Particles &p);  // capi.cpp
+void spec_from_box(const mdpd_box_spec &bs, Spec &s, Fill &fill);  // capi.cpp
 
 namespace {
 
@@ -187,10 +187,10 @@ JobFile read_job_file(const std::string &path)
         uint64_t bytes = 0;
         try {  // the checks a box of this spec meets at creation, with their messages
             Spec sp;
-            Particles p;
+            Fill fill;
             mdpd_box_spec one = b;
             one.n = 1;
-            spec_from_box(one, sp, p);
+            spec_from_box(one, sp, fill);
             bytes = Box::estimate_bytes(sp, b.n);
         } catch (const std::exception &ex) {
             bad(path, where, ex.what());

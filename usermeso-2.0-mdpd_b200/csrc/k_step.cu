@@ -11,6 +11,7 @@
 //   force (mdpd)   pair_mdpd_meso.cu:93-228
 //   force (dpd)    pair_dpd_meso.cu:91-205
 //   rebuild check  neighbor.cpp:1216-1231 (decide), :1244-1322 (check_distance)
+#include "engine.h"
 #include "kernels.h"
 #include "pair.cuh"
 
@@ -644,6 +645,64 @@ __global__ void k_load_state(const double *__restrict__ xa, const double *__rest
     if (tag) tag[i] = i + 1;
     if (type) type[i] = 1;
     if (mask) mask[i] = 1;
+}
+
+// splitmix64's output function (Steele, Lea and Flood, 2014): a counter-based hash
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// uniform in (0, 1) from draw k of the stream seed
+__device__ __forceinline__ double unit_open(unsigned long long seed, unsigned long long k)
+{
+    return ((double)(mix64(seed ^ mix64(k)) >> 11) + 0.5) * 0x1p-53;
+}
+
+// particle i: draws 16 i .. 16 i + 8 (x, y, z, then a Box-Muller pair per velocity component);
+// the velocity sum in 2^-32 fixed point (integer adds: the same total in any order)
+__global__ void k_fill(Fill f, double3 blo, double3 bhi, int n, double *__restrict__ xa, double *__restrict__ va,
+                       unsigned long long *mom)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    long long q[3] = {0, 0, 0};
+    if (i < n) {
+        const double lo[3] = {blo.x, blo.y, blo.z}, hi[3] = {bhi.x, bhi.y, bhi.z};
+        const unsigned long long k0 = 16ull * (unsigned long long)i;
+        for (int d = 0; d < 3; ++d) {
+            double x = f.lo[d] + unit_open(f.seed, k0 + d) * (f.hi[d] - f.lo[d]);
+            if (x >= hi[d]) x = lo[d];
+            xa[3 * (size_t)i + d] = x;
+            const double u1 = unit_open(f.seed, k0 + 3 + 2 * d), u2 = unit_open(f.seed, k0 + 4 + 2 * d);
+            const double v = f.vscale * sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+            va[3 * (size_t)i + d] = v;
+            q[d] = __double2ll_rn(v * 4294967296.0);
+        }
+    }
+    for (int d = 0; d < 3; ++d) {
+        for (int o = 16; o > 0; o >>= 1) q[d] += __shfl_xor_sync(0xffffffffu, q[d], o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(mom + d, (unsigned long long)q[d]);
+    }
+}
+
+__global__ void k_fill_center(int n, double *__restrict__ va, const unsigned long long *mom)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int d = 0; d < 3; ++d) va[3 * (size_t)i + d] -= (double)(long long)mom[d] * 0x1p-32 / n;
+}
+
+void launch_fill(cudaStream_t s, const Fill &f, const double box_lo[3], const double box_hi[3], int n, double *xa,
+                 double *va, unsigned long long *mom)
+{
+    if (n <= 0) return;
+    const int g = (n + 255) / 256;
+    k_fill<<<g, 256, 0, s>>>(f, make_double3(box_lo[0], box_lo[1], box_lo[2]),
+                             make_double3(box_hi[0], box_hi[1], box_hi[2]), n, xa, va, mom);
+    k_fill_center<<<g, 256, 0, s>>>(n, va, mom);
 }
 
 void launch_load_state(cudaStream_t s, const double *xa, const double *va, int n, double *const x[3],

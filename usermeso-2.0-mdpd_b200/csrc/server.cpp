@@ -23,7 +23,7 @@
 #include "script.h"
 
 namespace mdpd {
-void spec_from_box(const mdpd_box_spec &bs, Spec &s, Particles &p);
+void spec_from_box(const mdpd_box_spec &bs, Spec &s, Fill &fill);
 }
 
 using namespace mdpd;
@@ -136,17 +136,17 @@ void mdpd_server_s::loop()
         for (auto &j : admitted) {
             try {
                 Spec s;
-                Particles p;
+                Fill fill;
                 mdpd_box_spec bs = j->spec.box;
                 if (!j->x0.empty()) {
                     bs.x = j->x0.data();
                     bs.v = j->v0.empty() ? nullptr : j->v0.data();
                 }
-                spec_from_box(bs, s, p);
+                spec_from_box(bs, s, fill);
                 if (bs.x)
                     j->box.reset(new Box(s, bs.n, bs.x, bs.v, nullptr, nullptr, nullptr, cfg.sms));
                 else
-                    j->box.reset(new Box(s, p, cfg.sms));
+                    j->box.reset(new Box(s, bs.n, fill, cfg.sms));
                 std::lock_guard<std::mutex> lk(mu);
                 j->state = 1;
                 j->start_s = now();
@@ -278,11 +278,11 @@ int mdpd_box_bytes(const mdpd_box_spec *spec, uint64_t *bytes)
     if (!spec || !bytes || spec->n <= 0) return MDPD_ERR_ARG;
     try {
         Spec sp;
-        Particles p;
+        Fill fill;
         mdpd_box_spec bs = *spec;
         bs.x = nullptr, bs.v = nullptr;
         bs.n = 1;
-        spec_from_box(bs, sp, p);
+        spec_from_box(bs, sp, fill);
         *bytes = Box::estimate_bytes(sp, spec->n);
     } catch (const std::exception &) {
         return MDPD_ERR_ARG;
@@ -313,11 +313,11 @@ int mdpd_server_submit(mdpd_server_t *s, const mdpd_job_spec *job, int64_t *id)
     j->spec.box.v = nullptr;
     try {
         Spec sp;
-        Particles p;
+        Fill fill;
         mdpd_box_spec bs = job->box;
         bs.x = nullptr, bs.v = nullptr;
         bs.n = 1;  // geometry/physics check only; the footprint uses the real n
-        spec_from_box(bs, sp, p);
+        spec_from_box(bs, sp, fill);
         j->bytes = Box::estimate_bytes(sp, n);
     } catch (const std::exception &) {
         return MDPD_ERR_ARG;
