@@ -220,6 +220,19 @@ int mdpd_server_cancel(mdpd_server_t *s, int64_t job_id);
  * dissipative force then sees v at the full step once, where the running job had the half
  * step, so the continuation is statistically, not bitwise, the uninterrupted run) */
 int mdpd_server_preempt(mdpd_server_t *s, int64_t job_id);
+/* --- placement on the GPUs of a node ---------------------------------------------------------
+ * Assigns independent boxes (a batch spread over devices) or jobs (servers on several devices)
+ * to ndev devices: device_of[i] in [0, ndev), or -1 for an item that fits no device's
+ * budget_bytes[d] (MDPD_ERR_BUDGET is then returned; the others are still placed).  Work is
+ * specs[i].n * steps[i] (steps NULL: the particles, for boxes stepped together); items go in
+ * decreasing work to the device with the least work so far among those with room (longest
+ * processing time first; ties by index and by lower device), so every rank computes the same
+ * placement from the same list and no data crosses devices.  work_per_device (optional, ndev):
+ * the work placed on each.  Replaces the reference's static split of an ensemble into groups of
+ * case_size ranks per case (main_ensemble, src/main.cpp:49-117). */
+int mdpd_place(const mdpd_box_spec *specs, const int64_t *steps, int32_t nitem, int32_t ndev,
+               const uint64_t *budget_bytes, int32_t *device_of, double *work_per_device);
+
 /* JSON job specs: a file of boxes for one server,
  *   {"budget_gb": G, "timeout_s": T, "defaults": {<key>: value, ...},
  *    "jobs": [{"name": "a", "n": N, "box": L or [Lx, Ly, Lz], "steps": S, <key>: value, ...}]}
@@ -260,9 +273,13 @@ void mdpd_server_stop(mdpd_server_t *s);
  *   number of particles counted. Temperature in lj units is sums[0] / (3 sums[10] - 3).
  *   err (optional, err_len bytes): the reason for a non-zero return.
  * Limit: n <= 16,777,216 (2^24) per call; larger n returns MDPD_ERR_ARG without launching.
- * The first call on each device looks up the scratch array's device address with that
- * device current; make that first call before any stream capture. Every call on a device
- * shares the one scratch array: calls whose work overlaps on the GPU (two host threads on two
+ * The first call on each device looks up the scratch array's device address with that device
+ * current and keeps it for the life of the process; after a cudaDeviceReset of that device the
+ * kept address is stale, so a host that resets a device must not call this again in the same
+ * process. Every call copies the sums to pageable host memory and synchronises its stream: no
+ * call may be made while its stream (or, in global capture mode, any stream) is being captured,
+ * and one made on a capturing stream returns MDPD_ERR_ARG without launching. Every call on a
+ * device shares the one scratch array: calls whose work overlaps on the GPU (two host threads on two
  * streams, say) race and can return wrong sums, so run them one after another. Nothing needs
  * clearing between calls: each call writes every scratch entry it reads. */
 int mdpd_kinetic_sums_noalloc(const double *vx, const double *vy, const double *vz,

@@ -1,0 +1,55 @@
+"""The neighbour-list rebuild decision against the FP64 oracle engine (needs a B200).
+
+Neighbor::decide / check_distance (neighbor.cpp:1216-1322): with `neigh_modify every 1 delay 0
+check yes` a step rebuilds the list when some particle has moved more than skin/2 since the last
+build.  The device takes the exact maximum displacement in its integrate pass; the oracle engine
+loops over the particles.  From the same state, with the exact RNG (so the two trajectories agree
+to the FP32 rounding of the forces), both step one step at a time and the steps at which each
+rebuilt must be the same.
+"""
+import numpy as np
+import pytest
+
+import mdpd
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def build_steps(counts):
+    """steps (1-based) at which the build counter went up"""
+    c = np.asarray(counts)
+    return (np.nonzero(np.diff(c) > 0)[0] + 1).tolist()
+
+
+@pytest.mark.parametrize("style", [0, 1])
+def test_rebuild_steps_match_oracle_engine(style):
+    rng = np.random.default_rng(41 + style)
+    n, L = (6000, 10.0) if style == 0 else (3000, 10.0)
+    x = rng.uniform(0, L, (n, 3))
+    v = rng.normal(0, 1, (n, 3)); v -= v.mean(0)
+    kw = dict(seed=777, exact_rng=1) if style == 0 else dict(style=1, A=25.0, gamma=4.5, sigma=3.0, rho_est=0.0,
+                                                             seed=777, exact_rng=1)
+    # relax the random start on the GPU, then start both engines from the relaxed state
+    b = mdpd.Batch([mdpd.box_spec(n, L, x=x, v=v, **kw)])
+    b.setup()
+    b.step(200)
+    x0, v0 = b.state(0)
+    b.close()
+    b = mdpd.Batch([mdpd.box_spec(n, L, x=x0, v=v0, **kw)])
+    b.setup()
+    okw = dict(seed=777) if style == 0 else dict(style=1, a0=25.0, gamma=4.5, sigma=3.0, seed=777, rho_est=0.0)
+    sim = oracle.Sim(x0, v0, (0, 0, 0), (L, L, L), **okw)
+    sim.setup()
+    g, o = [b.thermo(0).nbuild], [sim.thermo()["nbuild"]]
+    for _ in range(40):
+        b.step(1)
+        sim.run(1)
+        g.append(b.thermo(0).nbuild)
+        o.append(sim.thermo()["nbuild"])
+    sim.close()
+    b.close()
+    sg, so = build_steps(g), build_steps(o)
+    print(f"\nstyle {style}: rebuild steps GPU {sg}, oracle {so}")
+    assert len(so) >= 5  # the window sees several builds
+    assert sg == so

@@ -1,5 +1,6 @@
-"""N>1 path of bench.py on CPU with gloo, world_size 2: each rank owns an independent box
-set (weak scaling, no data-path collective); only the timing/throughput reduction crosses
+"""N>1 path of bench.py on CPU with gloo, world_size 2: the weak-scaling box set (256 boxes per
+rank) is placed on the ranks by the library's mdpd_place, each rank computing the same placement
+and taking its share (no data-path collective); only the timing/throughput reduction crosses
 ranks (max of time, sum of particle-steps)."""
 import os
 import sys
@@ -17,8 +18,14 @@ def _worker(rank, world, port, out):
     from datetime import timedelta
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
     import bench
-    cfg = bench.config4(seed=1 + rank)
+    cfg = bench.rank_boxes(rank, world)
     ntot = sum(c["n"] for c in cfg)
+    # which boxes this rank took (seeds are unique per box): every rank sees every share
+    import torch
+    mine = torch.tensor(sorted(c["seed"] for c in cfg) + [-1] * (512 - len(cfg)), dtype=torch.int64)
+    shares = [torch.zeros_like(mine) for _ in range(world)]
+    dist.all_gather(shares, mine)
+    out["shares"] = [[int(x) for x in t if x >= 0] for t in shares]
     secs = 1.0 + rank  # rank 1 is the slow one
     value, tmax = bench.aggregate(ntot * 10, secs, world, device="cpu")
     out[rank] = (ntot, value, tmax)
@@ -33,7 +40,11 @@ def test_two_rank_weak_scaling_reduction():
     port = 29500 + os.getpid() % 1000
     mp.start_processes(_worker, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
     (n0, v0, t0), (n1, v1, t1) = out[0], out[1]
-    assert n0 != n1  # independent box sets per rank
+    import bench
+    every = sorted(c["seed"] for c in bench.config4(seed=1) + bench.config4(seed=2))
+    a, b = out["shares"]
+    assert not set(a) & set(b) and sorted(a + b) == every  # each box on exactly one rank
+    assert abs(n0 - n1) / (n0 + n1) < 0.01  # particles balanced between the ranks
     assert t0 == t1 == 2.0  # time is the max over ranks
     assert v0 == v1 == pytest.approx((n0 + n1) * 10 / 2.0)
 

@@ -474,10 +474,14 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__rest
 //           when it lies within the cutoff of the box bounding the bin's centres (the FP32
 //           bound is exact: each axis gap rounds to at most the gap to any centre, and the
 //           squared distance is monotone in the gaps), compacted into shared memory
-//           (x, y, z, j) -- about 3/4 of the candidates, the corners of the stencil drop out
-//   test    lane = kept candidate, loop over the centres: the ballot of centre c is the set of
-//           its hits in the round; a hit's lane writes it straight into c's row at c's count
-//           (held by lane c) plus its rank in the ballot, so rows fill in candidate order
+//           (x, y, z, j) -- about 3/4 of the candidates, the corners of the stencil drop out.
+//           On a reduced list a candidate below every centre of the batch (a smaller local
+//           index or a lower ghost image) is owned by none of them and can only be a hit within
+//           rn2_list, so it is kept only within that radius of the box
+//   test    two kept candidates per lane, loop over the centres: the ballots of centre c are
+//           the sets of its hits in the round; a hit's lane writes it straight into c's row at
+//           c's count (held by lane c) plus its rank in the ballots, so rows fill in candidate
+//           order
 // A hit is a pair within the cutoff, not the centre itself; on a box with list_reduce also
 // owned by the centre (a local above it, or an upper ghost image) or within rn2_list: the
 // other pairs can enter neither the density sum nor the pair-once force list before the next
@@ -572,6 +576,11 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
             const float lox = warp_min(is_c ? pc4.x : inf), hix = warp_max(is_c ? pc4.x : -inf);
             const float loy = warp_min(is_c ? pc4.y : inf), hiy = warp_max(is_c ? pc4.y : -inf);
             const float loz = warp_min(is_c ? pc4.z : inf), hiz = warp_max(is_c ? pc4.z : -inf);
+            // smallest centre index of the batch: a candidate below it (a local with a smaller
+            // index, or a lower ghost image) is owned by none of the centres, so on a reduced
+            // list it is a hit only within rn2, and the filter keeps it only within rn2 of the box
+            int cmin = is_c ? ci : 0x7fffffff;
+            for (int o = 16; o > 0; o >>= 1) cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
             int my_n = 0;  // lane c: entries of centre c so far
             int slot = 0;  // stencil slot of this lane's stream position (only grows)
             __syncwarp();
@@ -583,42 +592,52 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
                     bool keep = false;
                     float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
                     int j = 0;
+                    int up = 0;
                     if (q < total) {
                         // largest slot with s_cum[slot] <= q (s_cum[27] = total > q ends the walk)
                         while (s_cum[w][slot + 1] <= q) ++slot;
                         const int p = s_bs[w][slot] + (q - s_cum[w][slot]);
                         pj = B.bpos[p];
                         j = MDPD_IDX(B.bin_order[p], n_all(B));
+                        up = j >= nlocal && (pflags(pj) & kUpperImage) ? 1 << 30 : 0;
+                        const int key = j < nlocal ? j : (up ? 0x7fffffff : -1);
                         const float gx = fmaxf(fmaxf(lox - pj.x, pj.x - hix), 0.f);
                         const float gy = fmaxf(fmaxf(loy - pj.y, pj.y - hiy), 0.f);
                         const float gz = fmaxf(fmaxf(loz - pj.z, pj.z - hiz), 0.f);
-                        keep = dist2(gx, gy, gz) <= rc2;
+                        keep = dist2(gx, gy, gz) <= (key < cmin ? rn2 : rc2);
                     }
                     const unsigned kb = __ballot_sync(0xffffffffu, keep);
-                    const int up = j >= nlocal && (pflags(pj) & kUpperImage) ? 1 << 30 : 0;
                     if (keep) s_q[w][nk + __popc(kb & lt)] = make_float4(pj.x, pj.y, pj.z, __int_as_float(j | up));
                     nk += __popc(kb);
                 }
                 __syncwarp();
-                // test: lane = kept candidate, one ballot per centre, hits written at once
-                const int R = (nk + 31) >> 5;
-                for (int r = 0; r < R; ++r) {
-                    const int k = (r << 5) + lane;
-                    const bool live = k < nk;
-                    const float4 pj = live ? s_q[w][k] : make_float4(1e30f, 1e30f, 1e30f, 0.f);
+                // test: two kept candidates per lane (candidates k and k + 32 of a 64-candidate
+                // round), one ballot per centre and candidate, hits written at once; the second
+                // candidate's hits follow the first's in the row, so rows fill in candidate order
+                for (int r0 = 0; r0 < nk; r0 += 64) {
+                    const int ka = r0 + lane, kb2 = ka + 32;
+                    const float4 pa = ka < nk ? s_q[w][ka] : make_float4(1e30f, 1e30f, 1e30f, 0.f);
+                    const float4 pb = kb2 < nk ? s_q[w][kb2] : make_float4(1e30f, 1e30f, 1e30f, 0.f);
                     // ownership key: a local's index; an upper ghost image above every local,
                     // a lower one below
-                    const int jw = __float_as_int(pj.w), jv = jw & 0x3fffffff;
-                    const int key = jv < nlocal ? jv : (jw >> 30 ? 0x7fffffff : -1);
-#pragma unroll 4
+                    const int jwa = __float_as_int(pa.w), jva = jwa & 0x3fffffff;
+                    const int jwb = __float_as_int(pb.w), jvb = jwb & 0x3fffffff;
+                    const int keya = jva < nlocal ? jva : (jwa >> 30 ? 0x7fffffff : -1);
+                    const int keyb = jvb < nlocal ? jvb : (jwb >> 30 ? 0x7fffffff : -1);
+#pragma unroll 2
                     for (int c = 0; c < nc; ++c) {
                         const float4 cc = s_c[w][c];
                         const int cic = __float_as_int(cc.w);
-                        const float r2 = dist2(cc.x - pj.x, cc.y - pj.y, cc.z - pj.z);
-                        const bool hit = r2 <= rc2 && key != cic && (key > cic || r2 <= rn2);
-                        const unsigned bal = __ballot_sync(0xffffffffu, hit);
-                        list_put(table, ncol, cic, __shfl_sync(0xffffffffu, my_n, c), bal, lt, hit, jv);
-                        if (lane == c) my_n += __popc(bal);
+                        const float r2a = dist2(cc.x - pa.x, cc.y - pa.y, cc.z - pa.z);
+                        const float r2b = dist2(cc.x - pb.x, cc.y - pb.y, cc.z - pb.z);
+                        const bool hita = r2a <= rc2 && keya != cic && (keya > cic || r2a <= rn2);
+                        const bool hitb = r2b <= rc2 && keyb != cic && (keyb > cic || r2b <= rn2);
+                        const unsigned bala = __ballot_sync(0xffffffffu, hita);
+                        const unsigned balb = __ballot_sync(0xffffffffu, hitb);
+                        const int base = __shfl_sync(0xffffffffu, my_n, c);
+                        list_put(table, ncol, cic, base, bala, lt, hita, jva);
+                        list_put(table, ncol, cic, base + __popc(bala), balb, lt, hitb, jvb);
+                        if (lane == c) my_n += __popc(bala) + __popc(balb);
                     }
                 }
                 __syncwarp();

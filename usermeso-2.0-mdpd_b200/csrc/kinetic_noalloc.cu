@@ -116,7 +116,8 @@ int fail_cuda(char *err, int64_t err_len, const char *what, cudaError_t e)
 // g_kin_scratch itself to a kernel: on the host that name is only a stand-in for the device
 // symbol, so a kernel given it would fault or, where the GPU can reach host memory, silently
 // read and write the wrong memory. The address is looked up once per device, with that
-// device current, and cached.
+// device current, and cached for the life of the process (a cudaDeviceReset by the host
+// application invalidates it: the symbol may then live elsewhere).
 cudaError_t scratch_for_current_device(double **out)
 {
     int dev = 0;
@@ -181,6 +182,13 @@ extern "C" int mdpd_kinetic_sums_noalloc(const double *vx, const double *vy, con
                         "current device");
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the call ends by copying to pageable host memory and synchronising its stream, which a
+    // stream under capture cannot do: refuse rather than invalidate the caller's capture
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(s, &cap)) != cudaSuccess) return fail_cuda(err, err_len, "stream query", e);
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(err, err_len, MDPD_ERR_ARG,
+                    "mdpd_kinetic_sums_noalloc: the stream is being captured; call it outside any capture");
     const int nchunk = (int)((n + kChunk - 1) / kChunk);
     k_kinetic_chunks<<<nchunk, kThreads, 0, s>>>(vx, vy, vz, mass, mask, groupbit, (int)n, rows);
     k_kinetic_total<<<1, kThreads, 0, s>>>(nchunk, rows);

@@ -106,6 +106,8 @@ def lib():
             "mdpd_server_drain": ([vp, C.c_double], C.c_int),
             "mdpd_server_stats": ([vp, dp], C.c_int),
             "mdpd_server_stop": ([vp], None),
+            "mdpd_place": ([C.POINTER(BoxSpec), C.POINTER(C.c_int64), i32, i32, C.POINTER(C.c_uint64), i32p, dp],
+                           C.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -292,6 +294,23 @@ def box_spec(n, L, style=0, A=-40.0, B=25.0, gamma=4.5, kT=1.0, cut=1.0, cut_r=0
     s.fill_lo[:] = list(fill_lo); s.fill_hi[:] = list(fill_hi)
     s.start_step = int(start_step)
     return s
+
+
+def place(specs, ndev, budget_bytes, steps=None):
+    """device of each box or job (mdpd_place): work n * steps (steps None: n) balanced over ndev
+    devices under each device's budget; returns (device_of, work_per_device); a box that fits no
+    device gets -1 and raises MdpdError(ERR_BUDGET) unless every box was placed"""
+    n = len(specs)
+    arr = (BoxSpec * max(n, 1))(*specs)
+    st = None if steps is None else np.ascontiguousarray(steps, np.int64)
+    bud = np.ascontiguousarray(np.broadcast_to(np.asarray(budget_bytes, np.uint64), (ndev,)))
+    dev = np.zeros(max(n, 1), np.int32)
+    work = np.zeros(ndev)
+    rc = lib().mdpd_place(arr, _ptr(st, C.c_int64) if st is not None else None, n, ndev, _ptr(bud, C.c_uint64),
+                          _ptr(dev, C.c_int32), _ptr(work, C.c_double))
+    if rc:
+        raise MdpdError(rc, "mdpd_place: " + ("a box fits no device's budget" if rc == ERR_BUDGET else "bad argument"))
+    return dev[:n], work
 
 
 def box_bytes(spec):
