@@ -7,6 +7,9 @@
   python tests/golden/make_golden.py device <ref_device.json>
       gaussian_TEA<4> values and nvcc contraction probes produced on a B200 by
       `oracle/_ref/ref_pin device <ref_device.json>` -> ref_device.json.
+  python tests/golden/make_golden.py decks
+      the reference's example input decks, verbatim -> decks/ (the quasi-2D pore deck is
+      left out: its data file init_solids_fluids.dat is not in the reference tree)
 
 Reads the reference tree at REF (default /root/reference); nothing at test time does.
 """
@@ -52,6 +55,17 @@ def host():
         json.dump(prof, f, indent=1)
 
 
+DECKS = {"box_10x10x10/in.test": "in.test",
+         "liquid_vacuum_interface/in.gpu.water": "in.gpu.water",
+         "static_contact_angle_in_a_slit_nano_channel/in.gpu.static_contact": "in.gpu.static_contact"}
+
+
+def decks():
+    os.makedirs(os.path.join(HERE, "decks"), exist_ok=True)
+    for src, dst in DECKS.items():
+        shutil.copyfile(os.path.join(REF, "examples/v2.5", src), os.path.join(HERE, "decks", dst))
+
+
 def device(path):
     with open(path) as f:
         d = json.load(f)
@@ -62,5 +76,7 @@ def device(path):
 if __name__ == "__main__":
     if sys.argv[1] == "host":
         host()
+    elif sys.argv[1] == "decks":
+        decks()
     else:
         device(sys.argv[2])
