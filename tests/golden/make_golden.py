@@ -27,7 +27,7 @@ DECK = os.path.join(REF, "examples/v2.5/static_contact_angle_in_a_slit_nano_chan
 
 
 def host():
-    subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "ref"])
+    subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + REF])
     subprocess.check_call([os.path.join(ROOT, "oracle/_ref/ref_pin"), "host",
                            os.path.join(HERE, "tea_words.json")])
     # deck input (9,280 atoms) and reference outputs, verbatim
