@@ -89,7 +89,8 @@ void mdpd_destroy(mdpd_t *h);
  * locals+ghosts), "force" (float4, locals), "count" (int, locals), "tag" (int, locals),
  * "ghost_src" (int), "ghost_img" (int), "x" (double 3*n, locals, internal order),
  * "phi" (float, locals: wall volume fraction of fix aboundary/rho/meso),
- * "list" (int, n_col*ceil32(n): the locally transposed table, neigh_list_meso.cu:143-147; on an
+ * "list" (int, n_col*ceil32(n): the transposed table, entry k of particle i at
+ *   (i & ~31) * n_col + 32 k + (i & 31), like neigh_list_meso.cu:143-147 coalesced per warp; on an
  *   mDPD box without wall coupling or fix aboundary/meso its rows hold the owned pairs and those
  *   within r_d + skin + 1e-3, the rest of the reference's full list being unused there).
  * sizes: returns the element count of a field in *count.                                 */

@@ -318,7 +318,7 @@ int mdpd_get_pairs(mdpd_t *h, int32_t *ti, int32_t *tj, int64_t cap, int64_t *np
         int64_t np = 0;
         for (int i = 0; i < n; ++i)
             for (int k = 0; k < cnt[i]; ++k) {
-                const int j = table[(size_t)((i & ~31) + (k & 31)) * B.n_col + (k & ~31) + (i & 31)];
+                const int j = table[(size_t)(i & ~31) * B.n_col + 32 * k + (i & 31)];
                 if (np < cap && ti && tj) {
                     ti[np] = tag[i];
                     tj[np] = j < n ? tag[j] : tag[gsrc[j - n]];

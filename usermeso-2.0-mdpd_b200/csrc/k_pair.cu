@@ -54,7 +54,7 @@ template <bool HALF, int kGather> __device__ __forceinline__ void density_rows(c
     const float h = B.cut_rho, h2 = h * h, rcf2 = B.rc2_force;
     const int ncol = B.n_col, nlocal = B.nlocal;
     // unsigned 32-bit offsets: tables of up to 2^32 entries
-    const int *row = B.table + ((unsigned)(i & ~31) * (unsigned)ncol + (unsigned)(i & 31));  // entry k at (k & 31) * ncol + (k & ~31)
+    const int *row = B.table + ((unsigned)(i & ~31) * (unsigned)ncol + (unsigned)(i & 31));  // entry k at 32 k
     const int ncol2 = B.n_col2;
     int *row2 = B.table2 + (size_t)i * ncol2;
     float acc = 0.f;
@@ -65,7 +65,7 @@ template <bool HALF, int kGather> __device__ __forceinline__ void density_rows(c
 #pragma unroll
         for (int q = 0; q < kGather; ++q) {
             const int k = k0 + q;
-            j[q] = k < n ? MDPD_IDX(__ldcs(row + (k & 31) * ncol + (k & ~31)), n_all(B)) : -1;
+            j[q] = k < n ? MDPD_IDX(__ldcs(row + 32 * k), n_all(B)) : -1;
         }
 #pragma unroll
         for (int q = 0; q < kGather; ++q) pj[q] = j[q] >= 0 ? __ldg(&B.pos[j[q]]) : make_float4(1e30f, 0, 0, 0);

@@ -226,6 +226,17 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_cls(const BoxDesc *__restr
 // ---------------------------------------------------------------------------
 // R4 / R10: warp per bucket, order members by (sub key, index) or by index
 // ---------------------------------------------------------------------------
+// Position of particle i as the list build reads it from bpos: x, y, z and, in .w, its list word:
+// i for a local or an upper ghost image, ~i for a lower ghost image.  As a signed integer the word
+// orders a candidate against a centre (a local) as pair-once ownership does: a candidate whose
+// word is above the centre's index is owned by the centre (a local above it, or an upper image;
+// a lower image is negative, below every centre), and only the centre itself has an equal word.
+__device__ __forceinline__ float4 list_pos(const float4 &p, int i, int nlocal)
+{
+    const int wd = i < nlocal || (pflags(p) & kUpperImage) ? i : ~i;
+    return make_float4(p.x, p.y, p.z, __int_as_float(wd));
+}
+
 template <int MODE>  // 0: reorder classes -> perm, 1: bins -> bin_order + bpos
 __global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict__ boxes,
                                                    const Unit *__restrict__ units, int nunits)
@@ -273,7 +284,7 @@ __global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict_
                 for (int q = 0; q < n; ++q) rank += key[q] < k;
                 const int idx = (int)(uint32_t)k;
                 arr[s + rank] = idx;
-                if (MODE == 1) B.bpos[s + rank] = B.pos[idx];
+                if (MODE == 1) B.bpos[s + rank] = list_pos(B.pos[idx], idx, B.nlocal);
             }
             __syncwarp();
             if (lane == 0) cnt[b] = 0;
@@ -459,7 +470,7 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__rest
         int p;
         if (i < nl) {
             p = MDPD_IDX(B.bin_start[bin] + (i < B.st->n_bulk ? i - b0 : (b1 - b0) + (i - e0)), n_all(B));
-            B.bpos[p] = B.pos[i];
+            B.bpos[p] = list_pos(B.pos[i], i, nl);
         } else {
             const int nloc = (b1 - b0) + (B.cls_start[B.nbin + rk + 1] - e0);
             p = MDPD_IDX(atomicAdd(&B.bin_cursor[bin], 1) + nloc, n_all(B));
@@ -474,14 +485,15 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__rest
 //           when it lies within the cutoff of the box bounding the bin's centres (the FP32
 //           bound is exact: each axis gap rounds to at most the gap to any centre, and the
 //           squared distance is monotone in the gaps), compacted into shared memory
-//           (x, y, z, j) -- about 3/4 of the candidates, the corners of the stencil drop out.
-//           On a reduced list a candidate below every centre of the batch (a smaller local
-//           index or a lower ghost image) is owned by none of them and can only be a hit within
-//           rn2_list, so it is kept only within that radius of the box
-//   test    two kept candidates per lane, loop over the centres: the ballots of centre c are
-//           the sets of its hits in the round; a hit's lane writes it straight into c's row at
-//           c's count (held by lane c) plus its rank in the ballots, so rows fill in candidate
-//           order
+//           (x, y, z, list word; the particle index beside it).  On a reduced list a candidate
+//           below every centre of the batch (a smaller local index or a lower ghost image) is
+//           owned by none of them and can only be a hit within rn2_list, so it is kept only
+//           within that radius of the box
+//   test    two kept candidates per lane (k and k + 32 of a 64-candidate round), loop over the
+//           centres; the squared distances of both come from one two-lane FP32 evaluation
+//           (sub/mul/fma .f32x2, rounded per lane as the scalar dist2); the ballots of centre c
+//           are its hits in the round, and each hit's lane writes it straight into c's row at
+//           c's count plus its rank in the ballots, so rows fill in candidate order
 // A hit is a pair within the cutoff, not the centre itself; on a box with list_reduce also
 // owned by the centre (a local above it, or an upper ghost image) or within rn2_list: the
 // other pairs can enter neither the density sum nor the pair-once force list before the next
@@ -489,7 +501,7 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__rest
 // Work items are 8 bins (one per warp) of a 256-bin unit, taken grid-stride so every SM
 // stays full whatever the number of rebuilding boxes.
 // ---------------------------------------------------------------------------
-constexpr int kListChunk = 224;                 // kept candidates per chunk (7 rounds)
+constexpr int kListChunk = 224;                 // kept candidates per chunk (3.5 rounds)
 
 __device__ __forceinline__ float warp_min(float v)
 {
@@ -503,24 +515,47 @@ __device__ __forceinline__ float warp_max(float v)
     return v;
 }
 
-// hit of this lane for centre c (index cic, count so far base) into c's row
-__device__ __forceinline__ void list_put(int *table, int ncol, int cic, int base, unsigned bal,
-                                         unsigned lt, bool hit, int j)
+// two-lane FP32 arithmetic (sm_100a .f32x2): each lane rounds as the scalar instruction does
+__device__ __forceinline__ unsigned long long pk2(float a, float b)
 {
-    if (hit) {
-        const int p = base + __popc(bal & lt);
-        if (p < ncol)
-            table[(unsigned)(cic & ~31) * (unsigned)ncol + (unsigned)((cic & 31) + (p & 31) * ncol + (p & ~31))] = j;
-    }
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
 }
 
-// 4 blocks per SM: 64 registers and no spill, measured faster than 5 blocks at 48 with a spill
+__device__ __forceinline__ void upk2(unsigned long long r, float &a, float &b)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// dist2 on both lanes: fma(dz, dz, fma(dx, dx, dy * dy))
+__device__ __forceinline__ unsigned long long dist2x2(unsigned long long dx, unsigned long long dy,
+                                                      unsigned long long dz)
+{
+    unsigned long long t;
+    asm("mul.rn.f32x2 %0, %1, %1;" : "=l"(t) : "l"(dy));
+    asm("fma.rn.f32x2 %0, %1, %1, %0;" : "+l"(t) : "l"(dx));
+    asm("fma.rn.f32x2 %0, %1, %1, %0;" : "+l"(t) : "l"(dz));
+    return t;
+}
+
+// 4 blocks per SM: 64 registers
 __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ boxes,
                                                  const Unit *__restrict__ units, int nunits,
                                                  int nbox, int *done)
 {
-    __shared__ float4 s_c[8][32];                       // centre positions, index in .w
-    __shared__ float4 s_q[8][kListChunk];               // kept candidates: x, y, z, j | upper << 30
+    __shared__ float4 s_ca[8][32], s_cb[8][32];         // centres: x, x, y, y | z, z, index, row offset
+    __shared__ int s_n[8][32];                          // entries of each centre so far
+    __shared__ float4 s_q[8][kListChunk];               // kept candidates: x, y, z, list word
+    __shared__ int s_j[8][kListChunk];                  // their particle indices
+    __shared__ float4 s_lo[8], s_hi[8];                 // the centres' bounding box; cmin
     __shared__ int s_bs[8][32], s_cum[8][33];
     const int lane = threadIdx.x & 31, w = threadIdx.x / 32;
     const unsigned lt = (1u << lane) - 1u;
@@ -538,7 +573,7 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
         const float rc2 = B.rc2_tail;
         const float rn2 = B.list_reduce ? B.rn2_list : rc2;  // with rc2: every pair (full list)
         const int ncol = B.n_col, nlocal = B.nlocal;
-        int *table = B.table;
+        int *const table = B.table;
         const int bx = b % B.mbin[0], by = (b / B.mbin[0]) % B.mbin[1], bz = b / (B.mbin[0] * B.mbin[1]);
         // stencil bins: lane l < 27 takes offset (l%3-1, l/3%3-1, l/9-1)
         int st = 0, sz = 0;
@@ -571,78 +606,88 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
             if (cm == 0) break;
             const int nc = __popc(cm);
             const float4 pc4 = is_c ? B.bpos[pc] : make_float4(0.f, 0.f, 0.f, 0.f);
-            s_c[w][lane] = make_float4(pc4.x, pc4.y, pc4.z, __int_as_float(ci));
-            const float inf = __int_as_float(0x7f800000);
-            const float lox = warp_min(is_c ? pc4.x : inf), hix = warp_max(is_c ? pc4.x : -inf);
-            const float loy = warp_min(is_c ? pc4.y : inf), hiy = warp_max(is_c ? pc4.y : -inf);
-            const float loz = warp_min(is_c ? pc4.z : inf), hiz = warp_max(is_c ? pc4.z : -inf);
-            // smallest centre index of the batch: a candidate below it (a local with a smaller
-            // index, or a lower ghost image) is owned by none of the centres, so on a reduced
-            // list it is a hit only within rn2, and the filter keeps it only within rn2 of the box
-            int cmin = is_c ? ci : 0x7fffffff;
-            for (int o = 16; o > 0; o >>= 1) cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
-            int my_n = 0;  // lane c: entries of centre c so far
+            s_ca[w][lane] = make_float4(pc4.x, pc4.x, pc4.y, pc4.y);
+            // entry p of centre i at (i & ~31) * ncol + 32 p + (i & 31): entries p of 32
+            // consecutive centres are contiguous
+            s_cb[w][lane] = make_float4(pc4.z, pc4.z, __int_as_float(ci),
+                                        __uint_as_float((unsigned)(ci & ~31) * (unsigned)ncol + (unsigned)(ci & 31)));
+            s_n[w][lane] = 0;
+            {
+                const float inf = __int_as_float(0x7f800000);
+                const float lox = warp_min(is_c ? pc4.x : inf), hix = warp_max(is_c ? pc4.x : -inf);
+                const float loy = warp_min(is_c ? pc4.y : inf), hiy = warp_max(is_c ? pc4.y : -inf);
+                const float loz = warp_min(is_c ? pc4.z : inf), hiz = warp_max(is_c ? pc4.z : -inf);
+                // smallest centre index of the batch: a candidate below it (a local with a smaller
+                // index, or a lower ghost image) is owned by none of the centres, so on a reduced
+                // list it is a hit only within rn2, and the filter keeps it only within rn2 of the box
+                int cmin = is_c ? ci : 0x7fffffff;
+                for (int o = 16; o > 0; o >>= 1) cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
+                if (lane == 0) {
+                    s_lo[w] = make_float4(lox, loy, loz, __int_as_float(cmin));
+                    s_hi[w] = make_float4(hix, hiy, hiz, 0.f);
+                }
+            }
             int slot = 0;  // stencil slot of this lane's stream position (only grows)
             __syncwarp();
             for (int qs = 0; qs < total;) {
                 // filter: fill up to kListChunk kept candidates
                 int nk = 0;
+                const float4 lo = s_lo[w], hi = s_hi[w];
                 for (; qs < total && nk <= kListChunk - 32; qs += 32) {
                     const int q = qs + lane;
                     bool keep = false;
                     float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
-                    int j = 0;
-                    int up = 0;
                     if (q < total) {
                         // largest slot with s_cum[slot] <= q (s_cum[27] = total > q ends the walk)
                         while (s_cum[w][slot + 1] <= q) ++slot;
-                        const int p = s_bs[w][slot] + (q - s_cum[w][slot]);
-                        pj = B.bpos[p];
-                        j = MDPD_IDX(B.bin_order[p], n_all(B));
-                        up = j >= nlocal && (pflags(pj) & kUpperImage) ? 1 << 30 : 0;
-                        const int key = j < nlocal ? j : (up ? 0x7fffffff : -1);
-                        const float gx = fmaxf(fmaxf(lox - pj.x, pj.x - hix), 0.f);
-                        const float gy = fmaxf(fmaxf(loy - pj.y, pj.y - hiy), 0.f);
-                        const float gz = fmaxf(fmaxf(loz - pj.z, pj.z - hiz), 0.f);
-                        keep = dist2(gx, gy, gz) <= (key < cmin ? rn2 : rc2);
+                        pj = B.bpos[s_bs[w][slot] + (q - s_cum[w][slot])];
+                        const float gx = fmaxf(fmaxf(lo.x - pj.x, pj.x - hi.x), 0.f);
+                        const float gy = fmaxf(fmaxf(lo.y - pj.y, pj.y - hi.y), 0.f);
+                        const float gz = fmaxf(fmaxf(lo.z - pj.z, pj.z - hi.z), 0.f);
+                        keep = dist2(gx, gy, gz) <= (__float_as_int(pj.w) < __float_as_int(lo.w) ? rn2 : rc2);
                     }
                     const unsigned kb = __ballot_sync(0xffffffffu, keep);
-                    if (keep) s_q[w][nk + __popc(kb & lt)] = make_float4(pj.x, pj.y, pj.z, __int_as_float(j | up));
+                    if (keep) {
+                        const int k = nk + __popc(kb & lt);
+                        const int wd = __float_as_int(pj.w);
+                        s_q[w][k] = pj;
+                        s_j[w][k] = MDPD_IDX(wd ^ (wd >> 31), n_all(B));
+                    }
                     nk += __popc(kb);
                 }
                 __syncwarp();
-                // test: two kept candidates per lane (candidates k and k + 32 of a 64-candidate
-                // round), one ballot per centre and candidate, hits written at once; the second
-                // candidate's hits follow the first's in the row, so rows fill in candidate order
                 for (int r0 = 0; r0 < nk; r0 += 64) {
                     const int ka = r0 + lane, kb2 = ka + 32;
                     const float4 pa = ka < nk ? s_q[w][ka] : make_float4(1e30f, 1e30f, 1e30f, 0.f);
                     const float4 pb = kb2 < nk ? s_q[w][kb2] : make_float4(1e30f, 1e30f, 1e30f, 0.f);
-                    // ownership key: a local's index; an upper ghost image above every local,
-                    // a lower one below
-                    const int jwa = __float_as_int(pa.w), jva = jwa & 0x3fffffff;
-                    const int jwb = __float_as_int(pb.w), jvb = jwb & 0x3fffffff;
-                    const int keya = jva < nlocal ? jva : (jwa >> 30 ? 0x7fffffff : -1);
-                    const int keyb = jvb < nlocal ? jvb : (jwb >> 30 ? 0x7fffffff : -1);
-#pragma unroll 2
+                    const int ja = ka < nk ? s_j[w][ka] : 0, jb = kb2 < nk ? s_j[w][kb2] : 0;
+                    const int wa = __float_as_int(pa.w), wb = __float_as_int(pb.w);
+                    const unsigned long long px = pk2(pa.x, pb.x), py = pk2(pa.y, pb.y), pz = pk2(pa.z, pb.z);
+#pragma unroll 1
                     for (int c = 0; c < nc; ++c) {
-                        const float4 cc = s_c[w][c];
-                        const int cic = __float_as_int(cc.w);
-                        const float r2a = dist2(cc.x - pa.x, cc.y - pa.y, cc.z - pa.z);
-                        const float r2b = dist2(cc.x - pb.x, cc.y - pb.y, cc.z - pb.z);
-                        const bool hita = r2a <= rc2 && keya != cic && (keya > cic || r2a <= rn2);
-                        const bool hitb = r2b <= rc2 && keyb != cic && (keyb > cic || r2b <= rn2);
-                        const unsigned bala = __ballot_sync(0xffffffffu, hita);
-                        const unsigned balb = __ballot_sync(0xffffffffu, hitb);
-                        const int base = __shfl_sync(0xffffffffu, my_n, c);
-                        list_put(table, ncol, cic, base, bala, lt, hita, jva);
-                        list_put(table, ncol, cic, base + __popc(bala), balb, lt, hitb, jvb);
-                        if (lane == c) my_n += __popc(bala) + __popc(balb);
+                        const float4 A = s_ca[w][c], C = s_cb[w][c];
+                        const int cic = __float_as_int(C.z);
+                        float r2a, r2b;
+                        upk2(dist2x2(sub2(pk2(A.x, A.y), px), sub2(pk2(A.z, A.w), py), sub2(pk2(C.x, C.y), pz)),
+                             r2a, r2b);
+                        const bool ha = wa != cic && (r2a <= rn2 || (wa > cic && r2a <= rc2));
+                        const bool hb = wb != cic && (r2b <= rn2 || (wb > cic && r2b <= rc2));
+                        const unsigned bala = __ballot_sync(0xffffffffu, ha);
+                        const unsigned balb = __ballot_sync(0xffffffffu, hb);
+                        const int n0 = s_n[w][c];
+                        const int na = n0 + __popc(bala);
+                        // a row that would overflow keeps writing its last entry (the count
+                        // reports the overflow); the table holds ncol entries per row
+                        const unsigned row = __float_as_uint(C.w);
+                        if (ha) table[row + 32u * (unsigned)min(n0 + __popc(bala & lt), ncol - 1)] = ja;
+                        if (hb) table[row + 32u * (unsigned)min(na + __popc(balb & lt), ncol - 1)] = jb;
+                        s_n[w][c] = na + __popc(balb);  // every lane stores the same count
                     }
                 }
                 __syncwarp();
             }
             if (is_c) {
+                const int my_n = s_n[w][lane];
                 B.count[ci] = my_n < ncol ? my_n : ncol;
                 if (my_n > ncol) atomicOr(&B.st->status, kErrListOverflow);
                 local_max = max(local_max, my_n);

@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(kUnit *TPP, 16 / TPP) k_density(const BoxDesc 
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int k = k0 + q * TPP;
-                    j[q] = k < n ? MDPD_IDX(__ldcs(row + (k & 31) * ncol + (k & ~31)), n_all(B)) : -1;
+                    j[q] = k < n ? MDPD_IDX(__ldcs(row + 32 * k), n_all(B)) : -1;
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q) pj[q] = j[q] >= 0 ? __ldg(&B.pos[j[q]]) : make_float4(1e30f, 0, 0, 0);
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(kUnit *TPP, 8 / TPP) k_force(const BoxDesc *__
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const int k = kb + (b4 + q) * TPP;
-                        j[q] = k < n ? MDPD_IDX(__ldcs(row + (k & 31) * ncol + (k & ~31)), n_all(B)) : -1;
+                        j[q] = k < n ? MDPD_IDX(__ldcs(row + 32 * k), n_all(B)) : -1;
                     }
 #pragma unroll
                     for (int q = 0; q < 4; ++q)

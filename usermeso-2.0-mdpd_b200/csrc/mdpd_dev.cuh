@@ -100,7 +100,7 @@ struct BoxDesc {
     float4 *posrho;       // (x, y, z, rho) of locals then ghosts, written by the pair-once density pass
     float *phi[2];        // wall volume fraction of locals (double-buffered with x)
     int *gsrc, *gimg, *gfirst;
-    // ---- neighbour list (locally transposed: 32-row blocks) ----
+    // ---- neighbour list (transposed per 32 particles: entry k of i at (i&~31)*n_col + 32k + (i&31)) ----
     int *count, *table;
     // entries within the force cutoff whose source index is above the particle's (each pair
     // once), compacted by the density pass for the force pass
@@ -367,10 +367,11 @@ __host__ __device__ __forceinline__ int n_all(const BoxDesc &B)
     return B.nlocal + (B.st->nghost < B.ghost_cap ? B.st->nghost : B.ghost_cap);
 }
 
-// entry k of particle i in the locally transposed table
+// entry k of particle i in the locally transposed table: each group of 32 consecutive
+// particles owns 32 * n_col entries, entry k of its particles contiguous at 32 k
 __device__ __forceinline__ unsigned list_addr(int i, int k, int n_col)
 {
-    return (unsigned)((i & ~31) + (k & 31)) * (unsigned)n_col + (unsigned)((k & ~31) + (i & 31));
+    return (unsigned)(i & ~31) * (unsigned)n_col + (unsigned)(32 * k + (i & 31));
 }
 
 __device__ __forceinline__ int clamp_bin(int i, int nmax)

@@ -216,7 +216,7 @@ class Lammps:
         n = len(cnt)
         i = np.arange(n)[:, None]
         k = np.arange(ncol)[None, :]
-        addr = ((i & ~31) + (k & 31)) * ncol + (k & ~31) + (i & 31)
+        addr = (i & ~31) * ncol + 32 * k + (i & 31)
         rows = tab[addr]
         rows[k >= cnt[:, None]] = -1
         return cnt, rows
