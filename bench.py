@@ -14,8 +14,8 @@ mDPD box of N particles (rho 6.05, A -40, B 25, r_d 0.75, skin 0.3) stepped E ti
 in profile mode inside the NVTX range "prof" (integrate, rebuild, density and force as separate
 launches timed with CUDA events; `ncu --nvtx --nvtx-include "prof/"` selects them) and, with
 --rebuild, one forced full rebuild inside the range "rb".  --shape pins the density pass's
-neighbour gathers in flight (4, 6 or 8).  Prints one JSON line with the per-phase milliseconds
-and the graph step time.
+neighbour gathers in flight (4, 6 or 8), --force-shape the force pass's pair chains per warp (32
+or 64).  Prints one JSON line with the per-phase milliseconds and the graph step time.
 """
 import argparse
 import json
@@ -204,8 +204,8 @@ def profile_box(args):
     n = args.profile_box
     L = (n / RHO) ** (1 / 3)
     b = mdpd.Batch([mdpd.box_spec(n, L, A=-40.0, B=25.0, seed=4242, init_seed=99)])
-    if args.shape:
-        b.set_shapes(args.shape)
+    if args.shape or args.force_shape:
+        b.set_shapes(args.shape or 6, args.force_shape or 32)
     b.setup()
     b.step(args.equil)
     r0 = b.rebuild_steps()
@@ -235,6 +235,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip plain/served/roofline/cpu legs")
     ap.add_argument("--profile-box", type=int, default=0, help="profiling leg: one cubic box of this many particles")
     ap.add_argument("--shape", type=int, default=0, help="profiling leg: pinned density shape (4, 6, 8)")
+    ap.add_argument("--force-shape", type=int, default=0,
+                    help="profiling leg: pinned force shape (32: one pair chain per lane, 64: two)")
     ap.add_argument("--rebuild", action="store_true", help="profiling leg: one forced rebuild in the range rb")
     args = ap.parse_args()
     if args.profile_box:
@@ -265,7 +267,7 @@ def main():
     b = mdpd.Batch(specs, device=local)
     b.setup()
     b.step(args.equil)  # relax the random start (untimed)
-    shape_density, shape_force = b.tune()  # project autotuner (39 untimed steps)
+    shape_density, shape_force = b.tune()  # project autotuner (13 untimed steps per candidate shape)
     b.step(args.warmup)
     r0 = b.rebuild_steps()
     barrier()
@@ -288,13 +290,14 @@ def main():
             "vs_baseline": None, "dtype": "f32 pair / f64 integrate", "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD, "boxes": len(cfg), "particles_per_gpu": ntot,
                        "start": f"uniform random positions, Maxwell velocities, {args.equil} untimed steps, "
-                                "then the autotuner's 39 untimed steps",
+                                "then the autotuner's 13 untimed steps per candidate shape",
                        "rebuild_steps_timed": r1 - r0,
                        "l2": "inputs larger than L2: state + lists of ~%d particles (%.1f GB)" % (
                            ntot, ntot * 1.1e-6),
                        "parallelism": f"{world} GPU(s), {256 * world} boxes placed by mdpd_place "
                                       "(no data-path collective)",
-                       "tuned": {"density_gathers_in_flight": shape_density, "force_lanes_per_warp_share": shape_force}},
+                       "tuned": {"density_gathers_in_flight": shape_density,
+                                 "force_pair_chains_per_warp": shape_force}},
             "clocks": clk.summary(), "gpu_launches": gpu_launches}
 
     if not args.no_extras:
@@ -421,6 +424,7 @@ def main():
         wall = time.perf_counter() - t0
         res = [(srv.poll(j), n, steps) for j, n, steps in jobs]
         st = srv.stats()
+        tm = srv.timing()
         for j, _, _ in jobs:
             srv.cancel(j)
         srv.stop()
@@ -435,6 +439,7 @@ def main():
                           "particle_steps_offered": float(sum(n * steps for _, n, steps in jobs)),
                           "window_s": wall,
                           "served_over_plain": done_ps / wall / (plain_ps / plain_s),
+                          "loop_s": tm,
                           "sample": f"Poisson(20/s) droplet/slab jobs arriving over {SERVE_ARRIVE_S:.0f} s, N "
                                     "log-uniform 5k-2M, steps U{2000..20000}, 150 GB budget; throughput = "
                                     f"particle-steps done in the first {SERVE_WINDOW_S:.0f} s / wall time; job "

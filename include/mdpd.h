@@ -92,7 +92,8 @@ void mdpd_destroy(mdpd_t *h);
  * "list" (int, n_col*ceil32(n): the transposed table, entry k of particle i at
  *   (i & ~31) * n_col + 32 k + (i & 31), like neigh_list_meso.cu:143-147 coalesced per warp; on an
  *   mDPD box without wall coupling or fix aboundary/meso its rows hold the owned pairs and those
- *   within r_d + skin + 1e-3, the rest of the reference's full list being unused there).
+ *   within r_d + skin + 1e-3, the rest of the reference's full list being unused there; the
+ *   entries are particle indices: the device table's ownership flag in bit 31 is cleared).
  * sizes: returns the element count of a field in *count.                                 */
 int mdpd_field_size(mdpd_t *h, const char *name, int64_t *count);
 int mdpd_get_field(mdpd_t *h, const char *name, void *out, int64_t nbytes);
@@ -154,8 +155,9 @@ int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int
 /* project autotuner: times the candidate shapes of the pair passes on this batch (13 real steps
  * each, so the boxes advance) and keeps the fastest. Pair-once mDPD batches: *shape_density =
  * neighbour gathers in flight per lane in the density pass (4, 6 or 8), *shape_force = 32 (a
- * warp shares its 32 particles' pairs; fixed). Full-list batches (classic DPD, wall-coupled
- * mDPD): threads per particle of the density and force passes (1, 2 or 4 each). */
+ * warp shares its 32 particles' pairs out to its 32 lanes, one pair chain per lane) or 64 (two
+ * independent pair chains per lane; single-type batches only). Full-list batches (classic DPD,
+ * wall-coupled mDPD): threads per particle of the density and force passes (1, 2 or 4 each). */
 int mdpd_batch_tune(mdpd_batch_t *b, int32_t *shape_density, int32_t *shape_force);
 /* mdpd_batch_tune with its picks persisted in a JSON file (path; created when absent):
  * {"version": 1, "entries": {"<key>": {"density": D, "force": F, "ms_per_step": T}}}.  The key
@@ -252,6 +254,18 @@ int mdpd_jobs_validate(const char *spec_path, int32_t *njobs, uint64_t *bytes);
 int mdpd_run_jobs(const char *spec_path, const char *out_path, const mdpd_opts *opts);
 /* wait until every submitted job is done, failed or cancelled (timeout_s <= 0: no limit) */
 int mdpd_server_drain(mdpd_server_t *s, double timeout_s);
+/* the stepping set: between chunks the server steps, of its resident jobs, those with the least
+ * remaining work (particles x steps left) up to n particles together (always at least one job);
+ * the others wait on the device.  The set is picked again when a job of it ends, when a waiting
+ * job fits beside it, or when a waiting job has less than half the remaining work of its longest
+ * job.  n = 0 steps every resident job.  Default 8,388,608: a step over that many particles runs
+ * near full throughput on a B200, and a short job that arrives behind long ones is done in its own
+ * time.  No counterpart in the reference (one LAMMPS run per rank group, src/main.cpp:49-117). */
+int mdpd_server_set_step_particles(mdpd_server_t *s, int64_t n);
+/* where the serving loop's time went (6 doubles): host seconds creating boxes, forming batches
+ * (work units and captured step graphs), setting up new boxes, running chunks; device seconds of
+ * the chunks; number of batches formed */
+int mdpd_server_timing(mdpd_server_t *s, double *out6);
 /* throughput/latency summary: particle-steps/s, step p50/p99 ms, job p50/p99 s,
  * jobs done, peak resident bytes (7 doubles) */
 int mdpd_server_stats(mdpd_server_t *s, double *out7);

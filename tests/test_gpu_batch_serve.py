@@ -21,8 +21,10 @@ def specs():
     return out
 
 
-def run_alone(spec, steps):
+def run_alone(spec, steps, force_shape=32):
     b = mdpd.Batch([spec])
+    if force_shape != 32:
+        b.set_shapes(6, force_shape)
     b.setup()
     b.step(steps)
     x, v = b.state(0)
@@ -31,14 +33,17 @@ def run_alone(spec, steps):
     return x, v, t
 
 
-def test_batch_equals_alone_bitwise():
+@pytest.mark.parametrize("force_shape", [32, 64])
+def test_batch_equals_alone_bitwise(force_shape):
+    # both force-pass shapes (one or two pair chains per lane)
     sp = specs()
     steps = 120
     b = mdpd.Batch(sp)
+    b.set_shapes(6, force_shape)
     b.setup()
     b.step(steps)
     for k, s in enumerate(sp):
-        xa, va, ta = run_alone(s, steps)
+        xa, va, ta = run_alone(s, steps, force_shape)
         xb, vb = b.state(k)
         assert np.array_equal(xa, xb) and np.array_equal(va, vb), k
         assert b.thermo(k).nbuild == ta.nbuild
@@ -76,6 +81,35 @@ def test_server_continuous_batching_matches_alone():
     srv.stop()
 
 
+def test_server_steps_least_remaining_work_first():
+    # with a step cap below the long job's size plus the short one's, a short job that arrives
+    # while a long one runs steps alone until it is done (least remaining work first), then the
+    # long one goes on; a job cancelled while it waits leaves without stepping; every result is
+    # bitwise the run alone
+    sp = specs()
+    long_s, short_s, third = sp[3], sp[0], sp[1]
+    alone_long = run_alone(long_s, 3000)
+    alone_short = run_alone(short_s, 30)
+    srv = mdpd.Server(budget_bytes=int(20e9))
+    srv.set_step_particles(8000)
+    jl = srv.submit(long_s, 3000, keep_state=True)
+    time.sleep(0.2)  # the long job is under way
+    js = srv.submit(short_s, 30, keep_state=True)
+    jc = srv.submit(third, 100000)
+    srv.cancel(jc)
+    srv.drain(timeout_s=300)
+    rl, rs, rc = srv.poll(jl), srv.poll(js), srv.poll(jc)
+    assert rl.state == 2 and rs.state == 2 and rc.state == 4
+    assert rs.end_s < rl.end_s
+    assert rc.steps_done == 0
+    for jid, ref, n in ((jl, alone_long, long_s.n), (js, alone_short, short_s.n)):
+        x, v = srv.state(jid, n)
+        assert np.array_equal(x, ref[0]) and np.array_equal(v, ref[1])
+    with pytest.raises(mdpd.MdpdError):
+        srv.set_step_particles(-1)
+    srv.stop()
+
+
 def test_server_refuses_oversized_and_cancels():
     srv = mdpd.Server(budget_bytes=int(5e8))
     big = mdpd.box_spec(2_000_000, (2e6 / 6.05) ** (1 / 3))
@@ -102,7 +136,7 @@ def test_autotuner_picks_a_shape_and_keeps_the_physics():
     b.setup()
     b.step(20)
     g, f = b.tune()
-    assert g in (4, 6, 8) and f == 32
+    assert g in (4, 6, 8) and f in (32, 64)
     b.step(20)
     for k in range(4):
         t = b.thermo(k)
@@ -181,7 +215,7 @@ def test_tune_cache_persists_the_pick(tmp_path):
     b = mdpd.Batch(sp)
     b.setup()
     d, f, hit = b.tune(cache=cache)
-    assert not hit and d in (4, 6, 8) and f == 32
+    assert not hit and d in (4, 6, 8) and f in (32, 64)
     assert b.thermo(0).step == 39  # three candidates, 13 timed steps each
     doc = json.loads(cache.read_text())
     (key, entry), = doc["entries"].items()

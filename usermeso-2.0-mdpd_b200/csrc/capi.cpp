@@ -269,7 +269,11 @@ int mdpd_get_field(mdpd_t *h, const char *name, void *out, int64_t nbytes)
         else if (f == "phi") get(B.phi[c], 4);
         else if (f == "ghost_src") get(B.gsrc, 4);
         else if (f == "ghost_img") get(B.gimg, 4);
-        else if (f == "list") get(B.table, 4);
+        else if (f == "list") {  // indices only: the ownership flag of reduced rows is cleared
+            get(B.table, 4);
+            int32_t *o = static_cast<int32_t *>(out);
+            for (size_t q = 0; q < cnt; ++q) o[q] &= kEntryIndexMask;
+        }
         else if (f == "x" || f == "v") {
             if (cnt * 8 > nbytes) throw ScriptError(MDPD_ERR_ARG, "buffer too small");
             if (f == "x") b->download_state((double *)out, nullptr, nullptr, nullptr, nullptr, nullptr);
@@ -318,7 +322,7 @@ int mdpd_get_pairs(mdpd_t *h, int32_t *ti, int32_t *tj, int64_t cap, int64_t *np
         int64_t np = 0;
         for (int i = 0; i < n; ++i)
             for (int k = 0; k < cnt[i]; ++k) {
-                const int j = table[(size_t)(i & ~31) * B.n_col + 32 * k + (i & 31)];
+                const int j = table[(size_t)(i & ~31) * B.n_col + 32 * k + (i & 31)] & kEntryIndexMask;
                 if (np < cap && ti && tj) {
                     ti[np] = tag[i];
                     tj[np] = j < n ? tag[j] : tag[gsrc[j - n]];
@@ -542,12 +546,15 @@ int mdpd_batch_time(mdpd_batch_t *b, int64_t nsteps, double *ms)
 static std::vector<StepConfig> tune_candidates(const StepConfig &base)
 {
     std::vector<StepConfig> cands;
-    if (base.half) {  // pair-once passes: the density pass's gathers in flight
-        for (int g : {4, 6, 8}) {
-            StepConfig c = base;
-            c.gather = g;
-            cands.push_back(c);
-        }
+    if (base.half) {  // pair-once passes: the density pass's gathers in flight, the force pass's
+                      // pair chains per lane (two on single-type batches)
+        for (int slots = 1; slots <= (base.uniform_types ? 2 : 1); ++slots)
+            for (int g : {4, 6, 8}) {
+                StepConfig c = base;
+                c.gather = g;
+                c.force_slots = slots;
+                cands.push_back(c);
+            }
     } else {  // full-list passes: threads per particle of each pass
         for (int td : {1, 2, 4})
             for (int tf : {1, 2, 4}) {
@@ -564,7 +571,7 @@ static TunePick pick_of(const StepConfig &c, double ms)
 {
     TunePick p;
     p.density = c.half ? c.gather : c.tpp_density;
-    p.force = c.half ? 32 : c.tpp_force;
+    p.force = c.half ? 32 * c.force_slots : c.tpp_force;
     p.ms_per_step = ms;
     return p;
 }

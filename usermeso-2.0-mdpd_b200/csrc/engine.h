@@ -126,8 +126,8 @@ public:
     Batch &operator=(const Batch &) = delete;
 
     void setup();                          // forced rebuild, density, force (no kick), thermo partials
-    // setup of the listed boxes only: rebuild flags set for them alone; the density and force
-    // passes rerun for all boxes, which reproduces the same forces for the others
+    // setup of the listed boxes only: rebuild, density and force passes over their units (the
+    // other boxes keep their state and forces)
     void setup_boxes(const std::vector<int> &which);
     void reconfigure(const StepConfig &c);  // new pair-pass shapes: recapture the step graphs
     // nsteps graph replays; with ev_last the last one also computes energy and virial (the

@@ -38,11 +38,30 @@ constexpr double kFixInv = 1.0 / 4294967296.0;
 constexpr int kEntryTypeShift = 27;              // compact entry: j | (type of j - 1) << 27
 constexpr int kEntryIndex = (1 << kEntryTypeShift) - 1;
 
+__device__ __forceinline__ int nlocal_of(const BoxDesc &B) { return B.nlocal; }
+
 // ---------------------------------------------------------------------------------------------
 // density pass, global indices
 // ---------------------------------------------------------------------------------------------
-template <bool HALF, int kGather> __device__ __forceinline__ void density_rows(const BoxDesc &B, const Unit &U)
+// approximate 1/sqrt(x), denormal inputs taken as 0 (which gives +inf)
+__device__ __forceinline__ float rsqrt_ftz(float x)
 {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// One lane per row; the geometry of entries goes two at a time through the two-lane FP32
+// instructions.  A term is (h - r)^2 with r = rsq * rsqrt(rsq), formed as t = rsq * rsqrt(rsq) - h
+// (one rounding; t is -(h - r) exactly) and min(t, 0)^2: pairs beyond the cutoff add 0, and so do the particle's own
+// entry and coincident particles (rsq = 0 gives 0 * inf = NaN, which min() drops; a denormal rsq
+// gives inf).  The reference skips rsq < 1e-20; here a normal rsq below 1e-20 (two particles
+// closer than 1e-10, whose FP32 coordinates are then both below ~1e-3 in magnitude) would add
+// h^2.  Rows are padded to the warp's longest with the particle itself.  Owned entries (bit 31,
+// set by the list build) within the force cutoff go to the compact row.
+template <int kGather, bool UNI> __device__ __forceinline__ void density_rows(const BoxDesc &B, const Unit &U)
+{
+    static_assert(kGather % 2 == 0, "entries are taken two at a time");
     const int i = U.begin + threadIdx.x;
     const bool live = i < U.end;
     const int c = B.st->cur;
@@ -50,73 +69,78 @@ template <bool HALF, int kGather> __device__ __forceinline__ void density_rows(c
     const int n = live ? MDPD_IDX(B.count[i], B.n_col + 1) : 0;
     int nmax = n;
     for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
-    const float4 pi = live ? B.pos[i] : make_float4(0, 0, 0, 0);
-    const float h = B.cut_rho, h2 = h * h, rcf2 = B.rc2_force;
-    const int ncol = B.n_col, nlocal = B.nlocal;
+    const int self = live ? i : U.begin;
+    const float4 pi = B.pos[self];
+    const float h = B.cut_rho, rcf2 = B.rc2_force;
+    const unsigned long long pix = pk2(pi.x, pi.x), piy = pk2(pi.y, pi.y), piz = pk2(pi.z, pi.z);
+    const unsigned long long nh = pk2(-h, -h);
+    const int ncol = B.n_col, ncol2 = B.n_col2;
     // unsigned 32-bit offsets: tables of up to 2^32 entries
     const int *row = B.table + ((unsigned)(i & ~31) * (unsigned)ncol + (unsigned)(i & 31));  // entry k at 32 k
-    const int ncol2 = B.n_col2;
-    int *row2 = B.table2 + (size_t)i * ncol2;
+    int *row2 = B.table2 + (size_t)self * ncol2;
+    // one FP32 sum in row order: the terms of entries beyond the cutoff are exact zeros, so a row
+    // and its filtered copy (full and reduced lists) give the same rho bit for bit
     float acc = 0.f;
     int n2 = 0;
     for (int k0 = 0; k0 < nmax; k0 += kGather) {
-        int j[kGather];
+        int e[kGather];
         float4 pj[kGather];
 #pragma unroll
-        for (int q = 0; q < kGather; ++q) {
-            const int k = k0 + q;
-            j[q] = k < n ? MDPD_IDX(__ldcs(row + 32 * k), n_all(B)) : -1;
-        }
+        for (int q = 0; q < kGather; ++q) e[q] = k0 + q < n ? __ldcs(row + 32 * (k0 + q)) : self;
 #pragma unroll
-        for (int q = 0; q < kGather; ++q) pj[q] = j[q] >= 0 ? __ldg(&B.pos[j[q]]) : make_float4(1e30f, 0, 0, 0);
+        for (int q = 0; q < kGather; ++q) pj[q] = __ldg(&B.pos[MDPD_IDX(e[q] & kEntryIndexMask, n_all(B))]);
 #pragma unroll
-        for (int q = 0; q < kGather; ++q) {
-            const float dx = pi.x - pj[q].x, dy = pi.y - pj[q].y, dz = pi.z - pj[q].z;
-            const float rsq = dist2(dx, dy, dz);
-            if (rsq < h2 && rsq >= 1e-20f) {
-                const float d = h - rsq * rsqrtf(rsq);  // FP32 rsqrt, as the reference
-                acc = __fmaf_rn(d, d, acc);
-            }
-            if (HALF) {
-                const int jj = j[q];
-                if (rsq < rcf2 && (jj < nlocal ? jj > i : (pflags(pj[q]) & kUpperImage) != 0)) {
-                    if (n2 < ncol2) row2[n2] = jj | (ptype(pj[q]) << kEntryTypeShift);
+        for (int q = 0; q < kGather; q += 2) {
+            const unsigned long long dx = sub2(pix, pk2(pj[q].x, pj[q + 1].x));
+            const unsigned long long dy = sub2(piy, pk2(pj[q].y, pj[q + 1].y));
+            const unsigned long long dz = sub2(piz, pk2(pj[q].z, pj[q + 1].z));
+            const unsigned long long rsq = dist2x2(dx, dy, dz);
+            float ra, rb;
+            upk2(rsq, ra, rb);
+            float ta, tb;
+            upk2(fma2(rsq, pk2(rsqrt_ftz(ra), rsqrt_ftz(rb)), nh), ta, tb);
+            ta = fminf(ta, 0.f);
+            tb = fminf(tb, 0.f);
+            acc = __fmaf_rn(ta, ta, acc);
+            acc = __fmaf_rn(tb, tb, acc);
+#pragma unroll
+            for (int h2 = 0; h2 < 2; ++h2) {
+                const int eq = e[q + h2];
+                if (eq < 0 && (h2 ? rb : ra) < rcf2) {
+                    const int j = eq & kEntryIndexMask;
+                    row2[min(n2, ncol2 - 1)] = UNI ? j : j | (ptype(pj[q + h2]) << kEntryTypeShift);
                     ++n2;
                 }
             }
         }
     }
-    if (HALF && live) {
+    if (live) {
         B.count2[i] = min(n2, ncol2);
         if (n2 > ncol2) atomicOr(&B.st->status, kErrList2Overflow);
-    }
-    if (HALF ? live : in_group) {
         // a particle outside the density group keeps its rho (not written, as in the reference),
         // but its packed position is refreshed like every other
         const float r = in_group ? (float)(B.mass[ptype(pi)] * B.rho_factor) * acc : B.rho[i];
         if (in_group) B.rho[i] = r;
-        if (HALF) B.posrho[i] = make_float4(pi.x, pi.y, pi.z, r);
+        B.posrho[i] = make_float4(pi.x, pi.y, pi.z, r);
         if (i >= B.st->n_bulk) {
             const int g1 = min(B.gfirst[i + 1], B.ghost_cap);
             for (int g = B.gfirst[i]; g < g1; ++g) {
-                if (in_group) B.rho[nlocal + g] = r;
-                if (HALF) {
-                    const float4 pg = B.pos[nlocal + g];
-                    B.posrho[nlocal + g] = make_float4(pg.x, pg.y, pg.z, r);
-                }
+                if (in_group) B.rho[nlocal_of(B) + g] = r;
+                const float4 pg = B.pos[nlocal_of(B) + g];
+                B.posrho[nlocal_of(B) + g] = make_float4(pg.x, pg.y, pg.z, r);
             }
         }
     }
 }
 
-template <bool HALF, int kGather>
+template <int kGather, bool UNI>
 __global__ void __launch_bounds__(128, density_blocks<kGather>()) k_density_rows(const BoxDesc *__restrict__ boxes,
                                                       const Unit *__restrict__ units, int nunits)
 {
     const int u = blockIdx.x;
     if (u >= nunits) return;
     const Unit U = units[u];
-    density_rows<HALF, kGather>(boxes[U.box], U);
+    density_rows<kGather, UNI>(boxes[U.box], U);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -292,6 +316,227 @@ __device__ __forceinline__ void force_pairs(const BoxDesc &B, const Unit &U, Row
     if (EV) ev_to_partial<EV>(B, U, ev, S.red);
 }
 
+// ---------------------------------------------------------------------------------------------
+// force pass, two pair chains per lane (single-type batches)
+// ---------------------------------------------------------------------------------------------
+// The lane's share [m0, m1) of the warp's concatenated compact rows is split in two halves, each
+// walked by its own slot; every iteration evaluates one pair of each slot, so two independent
+// TEA chains and two gathers are in flight per lane, and the pair arithmetic of the two goes
+// through the two-lane FP32 instructions.  Sums, ownership and partner atomics are those of
+// force_pairs, so forces agree with it to FP32 rounding and are as deterministic.
+struct Slot2 {
+    int r, rbeg, rend;          // row within the warp; its first entry and end in the concatenation
+    float4 pi, vi;
+    float rho;
+    long long ax, ay, az;
+};
+
+__device__ __forceinline__ void slot_flush(const Slot2 &q, RowsSmem &S, int wb)
+{
+    sadd64(&S.lo[0][wb + q.r], &S.hi[0][wb + q.r], q.ax);
+    sadd64(&S.lo[1][wb + q.r], &S.hi[1][wb + q.r], q.ay);
+    sadd64(&S.lo[2][wb + q.r], &S.hi[2][wb + q.r], q.az);
+}
+
+// move the slot to the row holding entry m (m >= q.rend), flushing the row it leaves
+__device__ __forceinline__ void slot_advance(Slot2 &q, RowsSmem &S, const int *P, int wb, int m)
+{
+    slot_flush(q, S, wb);
+    q.ax = q.ay = q.az = 0;
+    do {
+        ++q.r;
+        q.rbeg = q.rend;
+        q.rend = P[q.r + 1];
+    } while (m >= q.rend);
+    q.pi = S.pi[wb + q.r];
+    q.vi = S.vi[wb + q.r];
+    q.rho = S.rho[wb + q.r];
+}
+
+__device__ __forceinline__ void slot_start(Slot2 &q, RowsSmem &S, const int *P, int wb, int m)
+{
+    q.r = row_of(P, m);
+    q.rbeg = P[q.r];
+    q.rend = P[q.r + 1];
+    q.pi = S.pi[wb + q.r];
+    q.vi = S.vi[wb + q.r];
+    q.rho = S.rho[wb + q.r];
+    q.ax = q.ay = q.az = 0;
+}
+
+template <bool EXACT, bool EV>
+__device__ __forceinline__ void force_pairs2(const BoxDesc &B, const Unit &U, RowsSmem &S)
+{
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5, wb = t & ~31;
+    if (t == 0) S.coeff[0] = B.coeff[0];
+    const int i = U.begin + t;
+    const bool live = i < U.end;
+    int len = 0;
+    if (live) {
+        S.pi[t] = B.pos[i];
+        S.vi[t] = B.vel[i];
+        S.rho[t] = B.rho[i];
+        len = MDPD_IDX(B.count2[i], B.n_col2 + 1);
+    }
+    warp_prefix(len, lane, S.pre[w]);
+    for (int c = 0; c < 3; ++c) S.lo[c][t] = S.hi[c][t] = 0u;
+    __syncthreads();
+    const int *P = S.pre[w];
+    const int T = P[32];
+    const int i0 = U.begin + wb, nlocal = B.nlocal, ncol2 = B.n_col2;
+    const int m0 = (lane * T) >> 5, m1 = ((lane + 1) * T) >> 5;
+    const int na = (m1 - m0 + 1) >> 1, mb0 = m0 + na;  // slot a: [m0, mb0), slot b: [mb0, m1)
+    const float fix_max = B.fix_pair_max;
+    unsigned long long *fax = B.facc, *fay = B.facc + nlocal, *faz = B.facc + 2 * nlocal;
+    const PairCoeff cf = S.coeff[0];
+    const float dtis = B.dt_inv_sqrt;
+    // pair constants, both halves
+    const unsigned long long one2 = pk2(1.f, 1.f), m1_2 = pk2(-1.f, -1.f), mh2 = pk2(-0.5f, -0.5f);
+    const unsigned long long mic2 = pk2(-cf.inv_cut, -cf.inv_cut), micr2 = pk2(-cf.inv_cut_r, -cf.inv_cut_r);
+    const unsigned long long A2 = pk2(cf.A, cf.A), B2 = pk2(cf.B, cf.B), g2 = pk2(cf.gamma, cf.gamma);
+    const unsigned long long sd2 = pk2(cf.sigma * dtis, cf.sigma * dtis);
+    EvAcc ev = {0, 0, 0, 0, 0, 0, 0};
+    bool bad = false;
+    if (na > 0) {
+        Slot2 qa, qb;
+        slot_start(qa, S, P, wb, m0);
+        const bool has_b = mb0 < m1;
+        slot_start(qb, S, P, wb, has_b ? mb0 : m0);
+        for (int k = 0; k < na; ++k) {
+            const int ma = m0 + k, mb = mb0 + k;
+            const bool hb = mb < m1;
+            if (ma >= qa.rend) slot_advance(qa, S, P, wb, ma);
+            if (hb && mb >= qb.rend) slot_advance(qb, S, P, wb, mb);
+            const int ea = __ldcs(B.table2 + (size_t)(i0 + qa.r) * ncol2 + (ma - qa.rbeg));
+            const int eb = hb ? __ldcs(B.table2 + (size_t)(i0 + qb.r) * ncol2 + (mb - qb.rbeg)) : ea;
+            const int ja = MDPD_IDX(ea & kEntryIndex, n_all(B)), jb = MDPD_IDX(eb & kEntryIndex, n_all(B));
+            const float4 pja = __ldg(&B.posrho[ja]), pjb = __ldg(&B.posrho[jb]);
+            const float4 vja = __ldg(&B.vel[ja]), vjb = __ldg(&B.vel[jb]);
+            const int srca = ja < nlocal ? ja : MDPD_IDX(__ldg(&B.gsrc[ja - nlocal]), nlocal);
+            const int srcb = jb < nlocal ? jb : MDPD_IDX(__ldg(&B.gsrc[jb - nlocal]), nlocal);
+            const float4 vib = hb ? qb.vi : qa.vi;
+            const float4 pib = hb ? qb.pi : qa.pi;
+            const float rhob = hb ? qb.rho : qa.rho;
+            // geometry
+            const unsigned long long dx = sub2(pk2(qa.pi.x, pib.x), pk2(pja.x, pjb.x));
+            const unsigned long long dy = sub2(pk2(qa.pi.y, pib.y), pk2(pja.y, pjb.y));
+            const unsigned long long dz = sub2(pk2(qa.pi.z, pib.z), pk2(pja.z, pjb.z));
+            const unsigned long long rsq = dist2x2(dx, dy, dz);
+            float rsa, rsb;
+            upk2(rsq, rsa, rsb);
+            // hardware 1/sqrt refined by one Newton-Raphson step (as pair_core)
+            const unsigned long long y0 = pk2(rsqrt_ftz(rsa), rsqrt_ftz(rsb));
+            const unsigned long long ne = fma2(mul2(rsq, y0), y0, m1_2);  // -(1 - rsq y0^2)
+            const unsigned long long rinv = fma2(mul2(ne, mh2), y0, y0);
+            const unsigned long long r = mul2(rsq, rinv);
+            float ra, rb;
+            upk2(r, ra, rb);
+            const bool in_a = rsa < cf.cutsq && rsa >= 1e-20f && ra >= 1e-10f;
+            const bool in_b = hb && rsb < cf.cutsq && rsb >= 1e-20f && rb >= 1e-10f;
+            // random numbers of both pairs (TEA words of the two signatures)
+            float rna, rnb;
+            if (EXACT) {
+                rna = (float)gaussian_exact(__float_as_uint(qa.vi.w), __float_as_uint(vja.w));
+                rnb = (float)gaussian_exact(__float_as_uint(vib.w), __float_as_uint(vjb.w));
+            } else {
+                rna = gaussian_fast(__float_as_uint(qa.vi.w), __float_as_uint(vja.w));
+                rnb = gaussian_fast(__float_as_uint(vib.w), __float_as_uint(vjb.w));
+            }
+            const unsigned long long dvx = sub2(pk2(qa.vi.x, vib.x), pk2(vja.x, vjb.x));
+            const unsigned long long dvy = sub2(pk2(qa.vi.y, vib.y), pk2(vja.y, vjb.y));
+            const unsigned long long dvz = sub2(pk2(qa.vi.z, vib.z), pk2(vja.z, vjb.z));
+            const unsigned long long dot = fma2(dz, dvz, fma2(dy, dvy, mul2(dx, dvx)));
+            const unsigned long long wc = fma2(r, mic2, one2);
+            float wra, wrb;
+            upk2(fma2(r, micr2, one2), wra, wrb);
+            const unsigned long long wcr = pk2(fmaxf(wra, 0.f), fmaxf(wrb, 0.f));
+            const unsigned long long rs = add2(pk2(qa.rho, rhob), pk2(pja.w, pjb.w));
+            // (A wc + B (rho_i + rho_j) wcr) - gamma wc^2 (dr.dv)/r + sigma wc xi / sqrt(dt), over r
+            const unsigned long long cons = fma2(A2, wc, mul2(mul2(B2, rs), wcr));
+            const unsigned long long diss = mul2(mul2(mul2(mul2(g2, wc), wc), dot), rinv);
+            const unsigned long long rnd = mul2(mul2(sd2, wc), pk2(rna, rnb));
+            const unsigned long long fp = mul2(add2(sub2(cons, diss), rnd), rinv);
+            float fpa, fpb;
+            upk2(fp, fpa, fpb);
+            fpa = in_a ? fpa : 0.f;
+            fpb = in_b ? fpb : 0.f;
+            float fxa, fxb, fya, fyb, fza, fzb;
+            const unsigned long long fpp = pk2(fpa, fpb);
+            upk2(mul2(dx, fpp), fxa, fxb);
+            upk2(mul2(dy, fpp), fya, fyb);
+            upk2(mul2(dz, fpp), fza, fzb);
+            if (EV) {
+                float wca, wcb, rsa_, rsb_, dxa, dxb, dya, dyb, dza, dzb;
+                upk2(wc, wca, wcb);
+                upk2(rs, rsa_, rsb_);
+                upk2(dx, dxa, dxb);
+                upk2(dy, dya, dyb);
+                upk2(dz, dza, dzb);
+                const float wcra = fmaxf(wra, 0.f), wcrb = fmaxf(wrb, 0.f);
+                if (in_a) {
+                    ev.pe += cf.e_cut * wca * wca + cf.e_cut_r * rsa_ * wcra * wcra;
+                    ev.vxx += dxa * dxa * fpa, ev.vyy += dya * dya * fpa, ev.vzz += dza * dza * fpa;
+                    ev.vxy += dxa * dya * fpa, ev.vxz += dxa * dza * fpa, ev.vyz += dya * dza * fpa;
+                }
+                if (in_b) {
+                    ev.pe += cf.e_cut * wcb * wcb + cf.e_cut_r * rsb_ * wcrb * wcrb;
+                    ev.vxx += dxb * dxb * fpb, ev.vyy += dyb * dyb * fpb, ev.vzz += dzb * dzb * fpb;
+                    ev.vxy += dxb * dyb * fpb, ev.vxz += dxb * dzb * fpb, ev.vyz += dyb * dzb * fpb;
+                }
+            }
+            bad |= !(fabsf(fxa) < fix_max && fabsf(fya) < fix_max && fabsf(fza) < fix_max);
+            bad |= !(fabsf(fxb) < fix_max && fabsf(fyb) < fix_max && fabsf(fzb) < fix_max);
+            const long long qxa = to_fix(fxa), qya = to_fix(fya), qza = to_fix(fza);
+            const long long qxb = to_fix(fxb), qyb = to_fix(fyb), qzb = to_fix(fzb);
+            qa.ax += qxa, qa.ay += qya, qa.az += qza;
+            qb.ax += qxb, qb.ay += qyb, qb.az += qzb;  // zero when slot b is idle
+            const int da = srca - U.begin;
+            if ((unsigned)da < 128u) {
+                sadd64(&S.lo[0][da], &S.hi[0][da], -qxa);
+                sadd64(&S.lo[1][da], &S.hi[1][da], -qya);
+                sadd64(&S.lo[2][da], &S.hi[2][da], -qza);
+            } else {
+                atomicAdd(fax + srca, (unsigned long long)(-qxa));
+                atomicAdd(fay + srca, (unsigned long long)(-qya));
+                atomicAdd(faz + srca, (unsigned long long)(-qza));
+            }
+            if (hb) {
+                const int db = srcb - U.begin;
+                if ((unsigned)db < 128u) {
+                    sadd64(&S.lo[0][db], &S.hi[0][db], -qxb);
+                    sadd64(&S.lo[1][db], &S.hi[1][db], -qyb);
+                    sadd64(&S.lo[2][db], &S.hi[2][db], -qzb);
+                } else {
+                    atomicAdd(fax + srcb, (unsigned long long)(-qxb));
+                    atomicAdd(fay + srcb, (unsigned long long)(-qyb));
+                    atomicAdd(faz + srcb, (unsigned long long)(-qzb));
+                }
+            }
+        }
+        slot_flush(qa, S, wb);
+        if (has_b) slot_flush(qb, S, wb);
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&B.st->status, kErrNonFinite);
+    __syncthreads();
+    if (live) {
+        atomicAdd(fax + i, join64(S.lo[0][t], S.hi[0][t]));
+        atomicAdd(fay + i, join64(S.lo[1][t], S.hi[1][t]));
+        atomicAdd(faz + i, join64(S.lo[2][t], S.hi[2][t]));
+    }
+    if (EV) ev_to_partial<EV>(B, U, ev, S.red);
+}
+
+template <bool EXACT, bool EV>
+__global__ void __launch_bounds__(128, 6) k_force_pairs2(const BoxDesc *__restrict__ boxes,
+                                                         const Unit *__restrict__ units, int nunits)
+{
+    __shared__ RowsSmem S;
+    const int u = blockIdx.x;
+    if (u >= nunits) return;
+    const Unit U = units[u];
+    force_pairs2<EXACT, EV>(boxes[U.box], U, S);
+}
+
 // 7 blocks per SM (up to 72 registers, no spill) measured fastest against 6 and 8
 template <bool EXACT, bool EV, bool UNI>
 __global__ void __launch_bounds__(128, 7) k_force_pairs(const BoxDesc *__restrict__ boxes,
@@ -341,10 +586,18 @@ void launch_density_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, co
 {
     const int g = u.local.n;
     if (g <= 0) return;
-    switch (c.gather) {
-    case 4: k_density_rows<true, 4><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
-    case 8: k_density_rows<true, 8><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
-    default: k_density_rows<true, 6><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
+    if (c.uniform_types) {
+        switch (c.gather) {
+        case 4: k_density_rows<4, true><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
+        case 8: k_density_rows<8, true><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
+        default: k_density_rows<6, true><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
+        }
+    } else {
+        switch (c.gather) {
+        case 4: k_density_rows<4, false><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
+        case 8: k_density_rows<8, false><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
+        default: k_density_rows<6, false><<<g, 128, 0, s>>>(boxes, u.local.d, g); break;
+        }
     }
 }
 
@@ -358,7 +611,15 @@ void launch_force_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, cons
 {
     const int g = u.local.n;
     if (g <= 0) return;
-    if (c.exact_rng) {
+    if (c.force_slots == 2 && c.uniform_types) {
+        if (c.exact_rng) {
+            if (ev) k_force_pairs2<true, true><<<g, 128, 0, s>>>(boxes, u.local.d, g);
+            else k_force_pairs2<true, false><<<g, 128, 0, s>>>(boxes, u.local.d, g);
+        } else {
+            if (ev) k_force_pairs2<false, true><<<g, 128, 0, s>>>(boxes, u.local.d, g);
+            else k_force_pairs2<false, false><<<g, 128, 0, s>>>(boxes, u.local.d, g);
+        }
+    } else if (c.exact_rng) {
         if (ev) force_half<true, true, false>(s, boxes, u);
         else if (c.uniform_types) force_half<true, false, true>(s, boxes, u);
         else force_half<true, false, false>(s, boxes, u);

@@ -515,37 +515,6 @@ __device__ __forceinline__ float warp_max(float v)
     return v;
 }
 
-// two-lane FP32 arithmetic (sm_100a .f32x2): each lane rounds as the scalar instruction does
-__device__ __forceinline__ unsigned long long pk2(float a, float b)
-{
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-
-__device__ __forceinline__ void upk2(unsigned long long r, float &a, float &b)
-{
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
-}
-
-__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b)
-{
-    unsigned long long d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-
-// dist2 on both lanes: fma(dz, dz, fma(dx, dx, dy * dy))
-__device__ __forceinline__ unsigned long long dist2x2(unsigned long long dx, unsigned long long dy,
-                                                      unsigned long long dz)
-{
-    unsigned long long t;
-    asm("mul.rn.f32x2 %0, %1, %1;" : "=l"(t) : "l"(dy));
-    asm("fma.rn.f32x2 %0, %1, %1, %0;" : "+l"(t) : "l"(dx));
-    asm("fma.rn.f32x2 %0, %1, %1, %0;" : "+l"(t) : "l"(dz));
-    return t;
-}
-
 // 4 blocks per SM: 64 registers
 __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ boxes,
                                                  const Unit *__restrict__ units, int nunits,
@@ -572,6 +541,9 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
         if (B.bin_order[s] >= B.nlocal) continue;  // no locals in this bin
         const float rc2 = B.rc2_tail;
         const float rn2 = B.list_reduce ? B.rn2_list : rc2;  // with rc2: every pair (full list)
+        // a row marks the entries its centre owns with bit 31 (kOwnedEntry), which the pair-once
+        // density pass reads instead of re-deriving ownership per step; other readers mask it off
+        const int own = (int)kOwnedEntry;
         const int ncol = B.n_col, nlocal = B.nlocal;
         int *const table = B.table;
         const int bx = b % B.mbin[0], by = (b / B.mbin[0]) % B.mbin[1], bz = b / (B.mbin[0] * B.mbin[1]);
@@ -679,8 +651,10 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
                         // a row that would overflow keeps writing its last entry (the count
                         // reports the overflow); the table holds ncol entries per row
                         const unsigned row = __float_as_uint(C.w);
-                        if (ha) table[row + 32u * (unsigned)min(n0 + __popc(bala & lt), ncol - 1)] = ja;
-                        if (hb) table[row + 32u * (unsigned)min(na + __popc(balb & lt), ncol - 1)] = jb;
+                        if (ha)
+                            table[row + 32u * (unsigned)min(n0 + __popc(bala & lt), ncol - 1)] = ja | (wa > cic ? own : 0);
+                        if (hb)
+                            table[row + 32u * (unsigned)min(na + __popc(balb & lt), ncol - 1)] = jb | (wb > cic ? own : 0);
                         s_n[w][c] = na + __popc(balb);  // every lane stores the same count
                     }
                 }

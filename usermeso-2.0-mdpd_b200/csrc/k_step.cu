@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kUnit, integrate_blocks(WALL)) k_integrate(Box
                 const int n = MDPD_IDX(B.count[i], B.n_col + 1);
                 const float cp = B.cut_phi;
                 for (int k = 0; k < n; ++k) {
-                    const int j = MDPD_IDX(B.table[list_addr(i, k, B.n_col)], n_all(B));
+                    const int j = MDPD_IDX(B.table[list_addr(i, k, B.n_col)] & kEntryIndexMask, n_all(B));
                     const float4 pj = B.pos[j];
                     if (!(pflags(pj) & 2)) continue;
                     int s = j, code = 13;
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(kUnit) k_aboundary_meso(BoxDesc *__restrict__ 
         float rho_w = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
         const int n = MDPD_IDX(B.count[i], B.n_col + 1);
         for (int k = 0; k < n; ++k) {
-            const int j = MDPD_IDX(B.table[list_addr(i, k, B.n_col)], n_all(B));
+            const int j = MDPD_IDX(B.table[list_addr(i, k, B.n_col)] & kEntryIndexMask, n_all(B));
             const int mj = j < B.nlocal ? B.mask[c][j] : B.mask[c][MDPD_IDX(B.gsrc[j - B.nlocal], B.nlocal)];
             if (!(mj & B.ab_wall_bit)) continue;
             const float4 c2 = B.pos[j];
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(kUnit *TPP, 16 / TPP) k_density(const BoxDesc 
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int k = k0 + q * TPP;
-                    j[q] = k < n ? MDPD_IDX(__ldcs(row + 32 * k), n_all(B)) : -1;
+                    j[q] = k < n ? MDPD_IDX(__ldcs(row + 32 * k) & kEntryIndexMask, n_all(B)) : -1;
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q) pj[q] = j[q] >= 0 ? __ldg(&B.pos[j[q]]) : make_float4(1e30f, 0, 0, 0);
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(kUnit *TPP, 8 / TPP) k_force(const BoxDesc *__
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const int k = kb + (b4 + q) * TPP;
-                        j[q] = k < n ? MDPD_IDX(__ldcs(row + 32 * k), n_all(B)) : -1;
+                        j[q] = k < n ? MDPD_IDX(__ldcs(row + 32 * k) & kEntryIndexMask, n_all(B)) : -1;
                     }
 #pragma unroll
                     for (int q = 0; q < 4; ++q)

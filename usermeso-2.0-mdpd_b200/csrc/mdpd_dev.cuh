@@ -27,6 +27,11 @@ enum : int {
     kErrIndex = 64,         // check build: an index outside its array (the access was skipped)
 };
 
+// bit 31 of a neighbour-list entry: the row's centre owns the pair (j a local above the centre,
+// or an upper ghost image); the index is the entry & kEntryIndexMask
+constexpr unsigned kOwnedEntry = 0x80000000u;
+constexpr int kEntryIndexMask = 0x7FFFFFFF;
+
 struct PairCoeff {  // per type pair; FP32 pair arithmetic
     float cut, cutsq, inv_cut, cut_r, inv_cut_r;
     float A, B, gamma, sigma;  // mdpd: A (attractive), B (repulsive); dpd: A = a0
@@ -327,6 +332,59 @@ __device__ __forceinline__ float gaussian_fast(uint32_t si, uint32_t sj)
 __device__ __forceinline__ float dist2(float dx, float dy, float dz)
 {
     return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+}
+
+// ---------------------------------------------------------------------------
+// Two-lane FP32 arithmetic (sm_100a .f32x2 instructions): one instruction does the same
+// operation on two independent values held as one 64-bit register pair; each half rounds
+// exactly as the scalar instruction does.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long pk2(float a, float b)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+
+__device__ __forceinline__ void upk2(unsigned long long r, float &a, float &b)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// a * b + c on both halves, one rounding each
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// dist2 on both halves: fma(dz, dz, fma(dx, dx, dy * dy))
+__device__ __forceinline__ unsigned long long dist2x2(unsigned long long dx, unsigned long long dy,
+                                                      unsigned long long dz)
+{
+    return fma2(dz, dz, fma2(dx, dx, mul2(dy, dy)));
 }
 
 // ---------------------------------------------------------------------------

@@ -1,6 +1,9 @@
 // Serving loop: jobs (boxes + step counts) are admitted while their device footprint fits
-// the HBM budget, stay resident until done, and are stepped together by the batched graph.
-// Arrivals and retirements change the batch between chunks of steps (continuous batching).
+// the HBM budget and stay resident until done.  Between chunks of steps the resident jobs with
+// the least remaining work (particles x steps left) are picked, up to a particle cap, and stepped
+// together by the batched graph (continuous batching, shortest remaining work first): a GPU step
+// over that many particles already runs at full throughput, and a short job that arrives behind
+// long ones finishes in its own time instead of theirs.  The others wait on the device.
 // One driver thread issues all device work; submit/poll/cancel/preempt only touch the queue.
 // A preempted job leaves with its x, v (tag order) and step count kept on the host: its
 // checkpoint, from which a resubmitted box (start_step) continues the run.
@@ -44,6 +47,8 @@ struct Job {
     size_t bytes = 0;
     bool cancel = false;
     bool preempt = false;
+    bool set_up = false;  // its setup (rebuild, density and force passes) has run
+    double remaining() const { return (double)spec.box.n * (double)(spec.nsteps - done); }
 };
 
 double pct(std::vector<float> v, double p)
@@ -69,10 +74,16 @@ struct mdpd_server_s {
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
     // stats
     double particle_steps = 0, busy_s = 0;
+    // host wall seconds of the loop's parts: box creation, batch formation (units and captured
+    // graphs), setup of new boxes, stepping chunks (device time of the chunks is busy_s)
+    double t_create = 0, t_form = 0, t_setup = 0, t_chunks = 0;
+    int64_t n_forms = 0;
     std::vector<float> all_step_ms;
     std::vector<double> job_latency_s;
     uint64_t resident = 0, peak_resident = 0;
     int chunk = 50;
+    // particles stepped together (0: every resident job); see mdpd_server_set_step_particles
+    int64_t step_cap = 8ll << 20;
 
     double now() const
     {
@@ -80,7 +91,53 @@ struct mdpd_server_s {
     }
 
     void loop();
+    // a job leaves the device: result, checkpoint (kept x, v) and latency recorded, box freed
+    void retire(Job &j, const Thermo &t, int error, bool finished);
+    // active minus `gone`
+    static void drop(std::vector<std::shared_ptr<Job>> &active, const std::vector<std::shared_ptr<Job>> &gone)
+    {
+        std::vector<std::shared_ptr<Job>> keep;
+        for (auto &j : active)
+            if (std::find(gone.begin(), gone.end(), j) == gone.end()) keep.push_back(j);
+        active.swap(keep);
+    }
 };
+
+void mdpd_server_s::retire(Job &j, const Thermo &t, int error, bool finished)
+{
+    const bool fail = error != 0;
+    const bool preempted = j.preempt && !finished && !fail && !j.cancel;
+    mdpd_thermo_t out{};
+    out.step = t.step;
+    out.natoms = t.n;
+    out.nbuild = t.nbuild;
+    out.temp = t.temp;
+    out.press = t.press;
+    out.ke = 0.5 * t.ke_all;
+    for (int d = 0; d < 3; ++d) out.momentum[d] = t.mom[d];
+    for (int d = 0; d < 6; ++d) out.ptensor[d] = t.ptensor[d];
+    out.pe = t.pe;
+    out.surface_tension = t.surface_tension;
+    out.status = t.status;
+    std::vector<double> xf, vf;
+    if ((j.spec.keep_state || preempted) && !fail) {
+        const int n = j.box->n;
+        xf.resize(3 * (size_t)n);
+        vf.resize(3 * (size_t)n);
+        j.box->download_by_tag(xf.data(), vf.data());
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    j.thermo = out;
+    j.xf.swap(xf);
+    j.vf.swap(vf);
+    j.state = fail ? 3 : j.cancel ? 4 : preempted ? 5 : 2;
+    if (fail) j.error = error;
+    j.end_s = now();
+    if (!preempted && !j.cancel) job_latency_s.push_back(j.end_s - j.submit_s);  // a preempted job goes on elsewhere
+    resident -= j.bytes;
+    j.box.reset();
+    cv.notify_all();
+}
 
 // the kernels of a batch are chosen per batch (pair style, RNG mode): jobs step together only
 // when they share both
@@ -92,7 +149,8 @@ static bool same_family(const Job &a, const Job &b)
 void mdpd_server_s::loop()
 {
     cudaSetDevice(device);
-    std::vector<std::shared_ptr<Job>> active;
+    std::vector<std::shared_ptr<Job>> active;    // resident jobs
+    std::vector<std::shared_ptr<Job>> stepping;  // the jobs of `batch`, in id order
     std::unique_ptr<Batch> batch;
     StepConfig cfg;
     cfg.sms = sm_count();
@@ -132,7 +190,7 @@ void mdpd_server_s::loop()
             }
         }
         // allocate admitted boxes (outside the lock)
-        std::vector<int> fresh;
+        const double tc0 = now();
         for (auto &j : admitted) {
             try {
                 Spec s;
@@ -159,21 +217,103 @@ void mdpd_server_s::loop()
                 resident -= j->bytes;
             }
         }
+        t_create += now() - tc0;
         peak_resident = std::max(peak_resident, resident);
         if (active.empty()) continue;
-        const bool changed = !admitted.empty() || !batch;
-        if (changed) {
-            batch.reset();
+        // jobs cancelled or preempted while they wait leave at the step they reached
+        std::vector<std::shared_ptr<Job>> leaving;
+        for (auto &j : active)
+            if ((j->cancel || j->preempt) &&
+                std::find(stepping.begin(), stepping.end(), j) == stepping.end())
+                leaving.push_back(j);
+        if (!leaving.empty()) {
             std::vector<Box *> raw;
-            for (auto &j : active) raw.push_back(j->box.get());
-            cfg.style = active[0]->spec.box.style;
-            cfg.exact_rng = active[0]->spec.box.exact_rng != 0;
+            for (auto &j : leaving)
+                if (j->set_up) raw.push_back(j->box.get());
+            std::vector<Thermo> th;
+            if (!raw.empty()) {
+                try {
+                    Batch tb(raw, cfg);  // a batch over the leaving boxes that have stepped, for their thermo only
+                    tb.thermo(th);
+                } catch (const std::exception &) {
+                    th.assign(raw.size(), Thermo{});
+                }
+            }
+            size_t q = 0;
+            for (auto &j : leaving) {
+                Thermo t{};
+                if (j->set_up) t = th[q++];
+                else {  // never stepped: the state it was admitted with
+                    t.step = j->spec.box.start_step;
+                    t.n = j->spec.box.n;
+                }
+                retire(*j, t, 0, false);
+            }
+            drop(active, leaving);
+        }
+        if (active.empty()) continue;
+        // the stepping set: least remaining work first, up to step_cap particles (at least one job).
+        // It is picked again when it has lost a job, when a waiting job fits beside it, or when a
+        // waiting job has less than half the remaining work of the longest stepping one; otherwise
+        // it keeps stepping as it is (each new set costs a batch and its captured graphs)
+        int64_t cap;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            cap = step_cap;
+        }
+        bool repick = !batch || stepping.empty();
+        if (!repick) {
+            int64_t np = 0;
+            double longest = 0;
+            for (auto &j : stepping) {
+                np += j->spec.box.n;
+                longest = std::max(longest, j->remaining());
+            }
+            for (auto &j : active) {
+                if (std::find(stepping.begin(), stepping.end(), j) != stepping.end()) continue;
+                if (cap <= 0 || np + j->spec.box.n <= cap || j->remaining() < 0.5 * longest) {
+                    repick = true;
+                    break;
+                }
+            }
+        }
+        std::vector<std::shared_ptr<Job>> want = stepping;
+        if (repick) {
+            want.clear();
+            std::vector<std::shared_ptr<Job>> order(active);
+            std::sort(order.begin(), order.end(), [](const std::shared_ptr<Job> &a, const std::shared_ptr<Job> &b) {
+                const double ra = a->remaining(), rb = b->remaining();
+                return ra < rb || (ra == rb && a->id < b->id);
+            });
+            int64_t np = 0;
+            for (auto &j : order) {
+                if (!want.empty() && cap > 0 && np + j->spec.box.n > cap) continue;
+                want.push_back(j);
+                np += j->spec.box.n;
+            }
+            std::sort(want.begin(), want.end(),
+                      [](const std::shared_ptr<Job> &a, const std::shared_ptr<Job> &b) { return a->id < b->id; });
+        }
+        if (!batch || want != stepping) {
+            batch.reset();
+            stepping = want;
+            std::vector<Box *> raw;
+            std::vector<int> fresh;
+            for (size_t k = 0; k < stepping.size(); ++k) {
+                raw.push_back(stepping[k]->box.get());
+                if (!stepping[k]->set_up) fresh.push_back((int)k);
+            }
+            cfg.style = stepping[0]->spec.box.style;
+            cfg.exact_rng = stepping[0]->spec.box.exact_rng != 0;
             try {
+                const double tf0 = now();
                 batch.reset(new Batch(raw, cfg));
-                for (size_t k = 0; k < active.size(); ++k)
-                    if (std::find(admitted.begin(), admitted.end(), active[k]) != admitted.end())
-                        fresh.push_back((int)k);
+                const double tf1 = now();
                 batch->setup_boxes(fresh);
+                for (int k : fresh) stepping[k]->set_up = true;
+                t_form += tf1 - tf0;
+                t_setup += now() - tf1;
+                ++n_forms;
             } catch (const std::exception &e) {
                 std::lock_guard<std::mutex> lk(mu);
                 for (auto &j : active) {
@@ -183,86 +323,54 @@ void mdpd_server_s::loop()
                     j->box.reset();
                 }
                 active.clear();
+                stepping.clear();
                 batch.reset();
                 resident = 0;
                 continue;
             }
         }
-        // run a chunk: until the first job finishes, at most `chunk` steps
+        // run a chunk: until the first stepping job finishes, at most `chunk` steps
         int64_t k = chunk;
-        for (auto &j : active) k = std::min<int64_t>(k, j->spec.nsteps - j->done);
+        for (auto &j : stepping) k = std::min<int64_t>(k, j->spec.nsteps - j->done);
         k = std::max<int64_t>(k, 1);
         Range chunk_range("mdpd::server_chunk");
+        const double tk0 = now();
         cudaEventRecord(e0, batch->stream());
         batch->run(k, false, true);  // a retiring job's thermo reports its last step's energy and virial
         cudaEventRecord(e1, batch->stream());
         cudaEventSynchronize(e1);
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
-        std::string msg;
-        const int st = batch->status(msg);
         long long nparts = 0;
-        for (auto &j : active) nparts += j->box->n;
+        for (auto &j : stepping) nparts += j->box->n;
+        t_chunks += now() - tk0;
         {
             std::lock_guard<std::mutex> lk(mu);
             particle_steps += (double)nparts * k;
             busy_s += ms * 1e-3;
             for (int64_t q = 0; q < k; ++q) all_step_ms.push_back(ms / k);
         }
-        // retire finished / failed / cancelled jobs
-        std::vector<std::shared_ptr<Job>> keep;
-        bool retired = false;
+        // retire finished / failed / cancelled / preempted stepping jobs
+        std::vector<std::shared_ptr<Job>> out;
         std::vector<Thermo> th;
-        for (size_t q = 0; q < active.size(); ++q) {
-            auto &j = active[q];
+        for (size_t q = 0; q < stepping.size(); ++q) {
+            auto &j = stepping[q];
             const BoxState bst = j->box->state();
             j->done += k;
             for (int64_t s = 0; s < k; ++s) j->step_ms.push_back(ms / k);
             const bool fail = bst.status != 0;
             const bool finished = j->done >= j->spec.nsteps;
-            const bool preempted = j->preempt && !finished && !fail && !j->cancel;
-            if (finished || fail || j->cancel || preempted) {
+            if (finished || fail || j->cancel || j->preempt) {
                 if (th.empty()) batch->thermo(th);
-                Thermo t = th[q];
-                mdpd_thermo_t out{};
-                out.step = t.step;
-                out.natoms = t.n;
-                out.nbuild = t.nbuild;
-                out.temp = t.temp;
-                out.press = t.press;
-                out.ke = 0.5 * t.ke_all;
-                for (int d = 0; d < 3; ++d) out.momentum[d] = t.mom[d];
-                for (int d = 0; d < 6; ++d) out.ptensor[d] = t.ptensor[d];
-                out.pe = t.pe;
-                out.surface_tension = t.surface_tension;
-                out.status = t.status;
-                std::vector<double> xf, vf;
-                if ((j->spec.keep_state || preempted) && !fail) {
-                    const int n = j->box->n;
-                    xf.resize(3 * (size_t)n);
-                    vf.resize(3 * (size_t)n);
-                    j->box->download_by_tag(xf.data(), vf.data());
-                }
-                std::lock_guard<std::mutex> lk(mu);
-                j->thermo = out;
-                j->xf.swap(xf);
-                j->vf.swap(vf);
-                j->state = fail ? 3 : j->cancel ? 4 : preempted ? 5 : 2;
-                if (fail) j->error = (bst.status & kErrNonFinite) ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW;
-                j->end_s = now();
-                if (!preempted) job_latency_s.push_back(j->end_s - j->submit_s);  // a preempted job goes on elsewhere
-                resident -= j->bytes;
-                retired = true;
-            } else
-                keep.push_back(j);
+                retire(*j, th[q], !fail ? 0 : (bst.status & kErrNonFinite) ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW,
+                       finished);
+                out.push_back(j);
+            }
         }
-        (void)st;
-        if (retired) {
+        if (!out.empty()) {
             batch.reset();
-            for (auto &j : active)
-                if (std::find(keep.begin(), keep.end(), j) == keep.end()) j->box.reset();
-            active.swap(keep);
-            cv.notify_all();
+            stepping.clear();
+            drop(active, out);
         }
     }
     batch.reset();
@@ -404,6 +512,28 @@ int mdpd_server_drain(mdpd_server_t *s, double timeout_s)
             return MDPD_ERR_TIMEOUT;
     } else
         s->cv.wait(lk, [&] { return !pending(); });
+    return MDPD_OK;
+}
+
+int mdpd_server_set_step_particles(mdpd_server_t *s, int64_t n)
+{
+    if (!s || n < 0) return MDPD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->step_cap = n;
+    s->cv.notify_all();
+    return MDPD_OK;
+}
+
+int mdpd_server_timing(mdpd_server_t *s, double *o)
+{
+    if (!s || !o) return MDPD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    o[0] = s->t_create;
+    o[1] = s->t_form;
+    o[2] = s->t_setup;
+    o[3] = s->t_chunks;
+    o[4] = s->busy_s;
+    o[5] = (double)s->n_forms;
     return MDPD_OK;
 }
 

@@ -105,6 +105,8 @@ def lib():
             "mdpd_server_cancel": ([vp, i64], C.c_int),
             "mdpd_server_drain": ([vp, C.c_double], C.c_int),
             "mdpd_server_stats": ([vp, dp], C.c_int),
+            "mdpd_server_set_step_particles": ([vp, C.c_int64], C.c_int),
+            "mdpd_server_timing": ([vp, dp], C.c_int),
             "mdpd_server_stop": ([vp], None),
             "mdpd_place": ([C.POINTER(BoxSpec), C.POINTER(C.c_int64), i32, i32, C.POINTER(C.c_uint64), i32p, dp],
                            C.c_int),
@@ -446,6 +448,22 @@ class Server:
 
     def cancel(self, jid):
         lib().mdpd_server_cancel(self.h, jid)
+
+    def timing(self):
+        """seconds in box creation, batch formation, setup of new boxes and chunks (host), the
+        chunks' device seconds, and the number of batches formed"""
+        o = np.zeros(6)
+        rc = lib().mdpd_server_timing(self.h, _ptr(o, C.c_double))
+        if rc:
+            raise MdpdError(rc, "timing failed")
+        return dict(zip(["create_s", "form_s", "setup_s", "chunks_s", "busy_s", "forms"], o.tolist()))
+
+    def set_step_particles(self, n):
+        """particles stepped together: the resident jobs with the least remaining work, up to n
+        (0: every resident job)"""
+        rc = lib().mdpd_server_set_step_particles(self.h, C.c_int64(int(n)))
+        if rc:
+            raise MdpdError(rc, "bad step-particle cap")
 
     def preempt(self, jid):
         """checkpoint and release a job (state 5): state(jid, n) then returns its x, v and
