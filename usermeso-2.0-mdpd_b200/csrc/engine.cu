@@ -2,8 +2,6 @@
 // IF(rebuild){...} -> density -> force), setup and thermo.
 #include "engine.h"
 
-#include <array>
-#include <map>
 #include <mutex>
 
 #include <algorithm>
@@ -122,25 +120,6 @@ static cudaMemPool_t box_pool()
 
 // Morton rank of each bin of an mbin[0] x mbin[1] x mbin[2] grid (bins in x-major order), one
 // sort per grid shape for the life of the process: a batch of boxes repeats few shapes
-static const std::vector<int> &morton_ranks(const int mbin[3])
-{
-    static std::mutex mu;
-    static std::map<std::array<int, 3>, std::vector<int>> cache;
-    std::lock_guard<std::mutex> lock(mu);
-    std::vector<int> &rank = cache[{mbin[0], mbin[1], mbin[2]}];
-    if (rank.empty()) {
-        const int nbin = mbin[0] * mbin[1] * mbin[2];
-        std::vector<std::pair<uint64_t, int>> codes(nbin);
-        for (int z = 0, b = 0; z < mbin[2]; ++z)
-            for (int y = 0; y < mbin[1]; ++y)
-                for (int x = 0; x < mbin[0]; ++x, ++b) codes[b] = {morton3(x, y, z), b};
-        std::sort(codes.begin(), codes.end());
-        rank.resize(nbin);
-        for (int r = 0; r < nbin; ++r) rank[codes[r].second] = r;
-    }
-    return rank;
-}
-
 template <class T> T *Box::alloc(size_t count)
 {
     const size_t bytes_ = (std::max<size_t>(count, 1) * sizeof(T) + 255) & ~size_t(255);
@@ -376,11 +355,7 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
     bytes = arena_need_;
 
     // Morton rank of every bin: reorder buckets are visited in Morton order of their bin
-    {
-        const std::vector<int> &rank = morton_ranks(g.mbin);
-        // the cached ranks outlive the queued copy
-        check_cuda(cudaMemcpyAsync(B.bin_rank, rank.data(), sizeof(int) * nbin, cudaMemcpyHostToDevice, 0), "upload");
-    }
+    launch_bin_ranks(0, g.mbin, B.bin_rank);
     // initial state into buffer 0: the caller's AoS x and v (or a device fill of them) go to the
     // list table's space (unused until the first build, which writes every entry it later
     // reads), a kernel splits them into x, xh and v components and fills tags/types/masks that

@@ -31,8 +31,8 @@
 namespace mdpd {
 
 // the density pass keeps G neighbour positions in flight per lane (G = 4, 6 or 8, chosen per
-// batch by the autotuner); blocks per SM at 64 registers
-template <int G> constexpr int density_blocks() { return G <= 4 ? 8 : 7; }
+// batch by the autotuner); blocks per SM: 8 at up to 64 registers (G = 4, 6), 7 at up to 72 (G = 8)
+template <int G> constexpr int density_blocks() { return G <= 6 ? 8 : 7; }
 constexpr float kFixF = 4294967296.0f;           // 2^32
 constexpr double kFixInv = 1.0 / 4294967296.0;
 constexpr int kEntryTypeShift = 27;              // compact entry: j | (type of j - 1) << 27
@@ -69,6 +69,10 @@ template <int kGather, bool UNI> __device__ __forceinline__ void density_rows(co
     const int n = live ? MDPD_IDX(B.count[i], B.n_col + 1) : 0;
     int nmax = n;
     for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+    // the warp's rows are one contiguous block of the table (entry k of its 32 rows at 32 k): it
+    // is asked into L2 at once, so the entry loads after the first group wait on L2, not on DRAM
+    if ((threadIdx.x & 31) == 0 && nmax > 0)
+        prefetch_l2_bulk(B.table + (unsigned)(i & ~31) * (unsigned)B.n_col, 128u * (unsigned)nmax);
     const int self = live ? i : U.begin;
     const float4 pi = B.pos[self];
     const float h = B.cut_rho, rcf2 = B.rc2_force;
@@ -224,6 +228,7 @@ __device__ __forceinline__ void force_pairs(const BoxDesc &B, const Unit &U, Row
     const bool live = i < U.end;
     int len = 0;
     if (live) {
+        prefetch_l2(B.table2 + (size_t)i * B.n_col2);  // the row's first 32 entries: one line
         S.pi[t] = B.pos[i];
         S.vi[t] = B.vel[i];
         S.rho[t] = B.rho[i];

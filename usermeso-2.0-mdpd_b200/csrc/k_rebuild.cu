@@ -18,6 +18,8 @@
 //            ballot (atomic-free) straight into the locally transposed table, reduced rows on
 //            pair-once boxes (gpu_build_neighbor_list, neigh_build_meso.cu:17-127; layout
 //            neigh_list_meso.cu:143-147)
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace mdpd {
@@ -642,8 +644,10 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
                         float r2a, r2b;
                         upk2(dist2x2(sub2(pk2(A.x, A.y), px), sub2(pk2(A.z, A.w), py), sub2(pk2(C.x, C.y), pz)),
                              r2a, r2b);
-                        const bool ha = wa != cic && (r2a <= rn2 || (wa > cic && r2a <= rc2));
-                        const bool hb = wb != cic && (r2b <= rn2 || (wb > cic && r2b <= rc2));
+                        // owned candidates are hits within rc2, the others within rn2 (<= rc2)
+                        const bool oa = wa > cic, ob = wb > cic;
+                        const bool ha = r2a <= (oa ? rc2 : rn2) && wa != cic;
+                        const bool hb = r2b <= (ob ? rc2 : rn2) && wb != cic;
                         const unsigned bala = __ballot_sync(0xffffffffu, ha);
                         const unsigned balb = __ballot_sync(0xffffffffu, hb);
                         const int n0 = s_n[w][c];
@@ -652,9 +656,9 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
                         // reports the overflow); the table holds ncol entries per row
                         const unsigned row = __float_as_uint(C.w);
                         if (ha)
-                            table[row + 32u * (unsigned)min(n0 + __popc(bala & lt), ncol - 1)] = ja | (wa > cic ? own : 0);
+                            table[row + 32u * (unsigned)min(n0 + __popc(bala & lt), ncol - 1)] = ja | (oa ? own : 0);
                         if (hb)
-                            table[row + 32u * (unsigned)min(na + __popc(balb & lt), ncol - 1)] = jb | (wb > cic ? own : 0);
+                            table[row + 32u * (unsigned)min(na + __popc(balb & lt), ncol - 1)] = jb | (ob ? own : 0);
                         s_n[w][c] = na + __popc(balb);  // every lane stores the same count
                     }
                 }
@@ -685,6 +689,19 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
         }
         if (threadIdx.x == 0) *done = 0;
     }
+}
+
+__global__ void k_bin_ranks(int mx, int my, int mz, int *rank)
+{
+    const int nbin = mx * my * mz;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbin; b += gridDim.x * blockDim.x)
+        rank[b] = morton_rank(b % mx, (b / mx) % my, b / (mx * my), mx, my, mz);
+}
+
+void launch_bin_ranks(cudaStream_t s, const int mbin[3], int *rank)
+{
+    const int nbin = mbin[0] * mbin[1] * mbin[2];
+    k_bin_ranks<<<std::min((nbin + 255) / 256, 148 * 8), 256, 0, s>>>(mbin[0], mbin[1], mbin[2], rank);
 }
 
 void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int *done)

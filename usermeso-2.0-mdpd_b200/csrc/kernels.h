@@ -63,6 +63,8 @@ void launch_force_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, cons
 // and mask 1 into the arrays given (null: left as uploaded)
 void launch_load_state(cudaStream_t s, const double *xa, const double *va, int n, double *const x[3],
                        double *const xh[3], double *const v[3], int *tag, int *type, int *mask);
+// Morton rank of every bin of an mbin[0] x mbin[1] x mbin[2] grid (bin x + mx (y + my z))
+void launch_bin_ranks(cudaStream_t s, const int mbin[3], int *rank);
 // copies of every box's BoxState into out[nbox]
 void launch_gather_states(cudaStream_t s, const BoxDesc *boxes, int nbox, BoxState *out);
 // x, v (component arrays, internal order) -> xo[3n], vo[3n] in tag order (tags 1..n)

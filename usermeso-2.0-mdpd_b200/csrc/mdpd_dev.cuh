@@ -194,6 +194,31 @@ __host__ __device__ __forceinline__ uint64_t morton3(uint32_t x, uint32_t y, uin
     return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
 }
 
+// Rank of bin (x, y, z) among the bins of an mx x my x mz grid ordered by morton3: the bins
+// before it are counted octree level by level, from the top.  At level L the bin lies in an
+// octant (z bit, y bit, x bit of L) of a cube of side 2^(L+1); every octant of that cube with a
+// smaller index comes earlier in Morton order, with all of its bins that lie in the grid.  No
+// sort, so a device thread per bin ranks any grid shape.
+__host__ __device__ __forceinline__ int morton_rank(int x, int y, int z, int mx, int my, int mz)
+{
+    int top = 0;
+    while ((1 << top) < mx || (1 << top) < my || (1 << top) < mz) ++top;
+    long long rank = 0;
+    for (int L = top - 1; L >= 0; --L) {
+        const int size = 1 << L;
+        const int px = (x >> (L + 1)) << (L + 1), py = (y >> (L + 1)) << (L + 1), pz = (z >> (L + 1)) << (L + 1);
+        const int mine = (((z >> L) & 1) << 2) | (((y >> L) & 1) << 1) | ((x >> L) & 1);
+        for (int c = 0; c < mine; ++c) {
+            const int ox = px + (c & 1) * size, oy = py + ((c >> 1) & 1) * size, oz = pz + ((c >> 2) & 1) * size;
+            const long long cx = mx - ox < 0 ? 0 : (mx - ox > size ? size : mx - ox);
+            const long long cy = my - oy < 0 ? 0 : (my - oy > size ? size : my - oy);
+            const long long cz = mz - oz < 0 ? 0 : (mz - oz > size ? size : mz - oz);
+            rank += cx * cy * cz;
+        }
+    }
+    return (int)rank;
+}
+
 // seed of the current step: premix_TEA<64>(seed, step)
 __host__ __device__ __forceinline__ uint32_t seed_now(uint32_t seed, long long step)
 {
@@ -332,6 +357,18 @@ __device__ __forceinline__ float gaussian_fast(uint32_t si, uint32_t sj)
 __device__ __forceinline__ float dist2(float dx, float dy, float dz)
 {
     return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+}
+
+// Asks the memory system to bring [p, p + bytes) into L2 (a hint: no data returns, nothing waits
+// on it).  p 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void prefetch_l2_bulk(const void *p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void prefetch_l2(const void *p)
+{
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
 // ---------------------------------------------------------------------------
