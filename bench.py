@@ -203,7 +203,7 @@ def profile_box(args):
     import mdpd
     n = args.profile_box
     L = (n / RHO) ** (1 / 3)
-    b = mdpd.Batch([mdpd.box_spec(n, L, A=-40.0, B=25.0, seed=4242, init_seed=99)])
+    b = mdpd.Batch([mdpd.box_spec(n, L, A=-40.0, B=25.0, seed=4242, init_seed=99, exact_rng=int(args.exact))])
     if args.shape or args.force_shape:
         b.set_shapes(args.shape or 6, args.force_shape or 32)
     b.setup()
@@ -212,7 +212,8 @@ def profile_box(args):
     torch.cuda.nvtx.range_push("prof")
     p = b.profile(args.steps)
     torch.cuda.nvtx.range_pop()
-    out = {"particles": n, "shape": args.shape or "default", "profile_ms": p,
+    out = {"particles": n, "shape": args.shape or "default", "force_shape": args.force_shape or "default",
+           "rng": "exact" if args.exact else "fast", "profile_ms": p,
            "rebuild_steps": b.rebuild_steps() - r0}
     if args.rebuild:
         torch.cuda.synchronize()
@@ -238,6 +239,7 @@ def main():
     ap.add_argument("--force-shape", type=int, default=0,
                     help="profiling leg: pinned force shape (32: one pair chain per lane, 64: two)")
     ap.add_argument("--rebuild", action="store_true", help="profiling leg: one forced rebuild in the range rb")
+    ap.add_argument("--exact", action="store_true", help="profiling leg: FP64 bit-exact pair gaussian (rng exact)")
     args = ap.parse_args()
     if args.profile_box:
         profile_box(args)

@@ -206,6 +206,9 @@ typedef struct mdpd_job_result {
 
 /* device bytes a box of this spec holds while resident (the admission footprint) */
 int mdpd_box_bytes(const mdpd_box_spec *spec, uint64_t *bytes);
+/* starts the serving loop on opts->device. Before it returns, up to budget_bytes of device
+ * memory (no more than is free, less 2 GiB) is mapped into the library's box pool, which keeps
+ * it for the life of the process: admissions then take boxes without mapping fresh pages. */
 int mdpd_server_start(mdpd_server_t **s, uint64_t budget_bytes, const mdpd_opts *opts);
 int mdpd_server_submit(mdpd_server_t *s, const mdpd_job_spec *job, int64_t *job_id);
 int mdpd_server_poll(mdpd_server_t *s, int64_t job_id, mdpd_job_result *out);

@@ -118,8 +118,28 @@ static cudaMemPool_t box_pool()
     return pools[dev];
 }
 
-// Morton rank of each bin of an mbin[0] x mbin[1] x mbin[2] grid (bins in x-major order), one
-// sort per grid shape for the life of the process: a batch of boxes repeats few shapes
+size_t reserve_box_pool(size_t bytes)
+{
+    // one allocation of the whole size, freed back at once: the pool keeps the memory mapped
+    // (release threshold: never), so boxes created later take it without mapping new pages
+    cudaMemPool_t pool = box_pool();
+    cudaStream_t s;
+    check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+    size_t got = 0;
+    for (size_t want = bytes; want >= (size_t(1) << 30); want /= 2) {
+        void *p = nullptr;
+        if (cudaMallocFromPoolAsync(&p, want, pool, s) == cudaSuccess) {
+            check_cuda(cudaFreeAsync(p, s), "pool reserve");
+            got = want;
+            break;
+        }
+        cudaGetLastError();  // an out-of-memory answer is not left for the next caller
+    }
+    check_cuda(cudaStreamSynchronize(s), "pool reserve");
+    cudaStreamDestroy(s);
+    return got;
+}
+
 template <class T> T *Box::alloc(size_t count)
 {
     const size_t bytes_ = (std::max<size_t>(count, 1) * sizeof(T) + 255) & ~size_t(255);

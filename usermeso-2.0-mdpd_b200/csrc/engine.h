@@ -177,5 +177,8 @@ void check_cuda(cudaError_t e, const char *what);
 void launch_fill(cudaStream_t s, const Fill &f, const double box_lo[3], const double box_hi[3], int n, double *xa,
                  double *va, unsigned long long *mom);
 int sm_count();
+// maps up to `bytes` of device memory into the current device's box pool ahead of use (halving
+// the request until it fits, down to 1 GiB); returns the bytes reserved (0: none)
+size_t reserve_box_pool(size_t bytes);
 
 }  // namespace mdpd

@@ -404,6 +404,20 @@ int mdpd_server_start(mdpd_server_t **out, uint64_t budget, const mdpd_opts *opt
     auto *s = new mdpd_server_s;
     s->budget = budget;
     s->device = opts ? opts->device : 0;
+    // the budget's device memory is mapped into the box pool now, so an admission does not pay
+    // for mapping fresh pages (the pool keeps it for the process's later boxes too)
+    if (cudaSetDevice(s->device) != cudaSuccess) {
+        cudaGetLastError();
+        delete s;
+        return MDPD_ERR_CUDA;
+    }
+    try {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+            reserve_box_pool((size_t)std::min<uint64_t>(budget, free_b > (2ull << 30) ? free_b - (2ull << 30) : 0));
+    } catch (const std::exception &) {
+        cudaGetLastError();
+    }
     s->th = std::thread([s] { s->loop(); });
     *out = s;
     return MDPD_OK;
