@@ -14,8 +14,8 @@ mDPD box of N particles (rho 6.05, A -40, B 25, r_d 0.75, skin 0.3) stepped E ti
 in profile mode inside the NVTX range "prof" (integrate, rebuild, density and force as separate
 launches timed with CUDA events; `ncu --nvtx --nvtx-include "prof/"` selects them) and, with
 --rebuild, one forced full rebuild inside the range "rb".  --shape pins the density pass's
-neighbour gathers in flight (4, 6 or 8), --force-shape the force pass's pair chains per warp (32
-or 64).  Prints one JSON line with the per-phase milliseconds and the graph step time.
+neighbour gathers in flight (4, 6 or 8); --exact uses the FP64 bit-exact pair gaussian.  Prints
+one JSON line with the per-phase milliseconds and the graph step time.
 """
 import argparse
 import json
@@ -204,16 +204,16 @@ def profile_box(args):
     n = args.profile_box
     L = (n / RHO) ** (1 / 3)
     b = mdpd.Batch([mdpd.box_spec(n, L, A=-40.0, B=25.0, seed=4242, init_seed=99, exact_rng=int(args.exact))])
-    if args.shape or args.force_shape:
-        b.set_shapes(args.shape or 6, args.force_shape or 32)
+    if args.shape:
+        b.set_shapes(args.shape)
     b.setup()
     b.step(args.equil)
     r0 = b.rebuild_steps()
     torch.cuda.nvtx.range_push("prof")
     p = b.profile(args.steps)
     torch.cuda.nvtx.range_pop()
-    out = {"particles": n, "shape": args.shape or "default", "force_shape": args.force_shape or "default",
-           "rng": "exact" if args.exact else "fast", "profile_ms": p,
+    out = {"particles": n, "shape": args.shape or "default", "rng": "exact" if args.exact else "fast",
+           "profile_ms": p,
            "rebuild_steps": b.rebuild_steps() - r0}
     if args.rebuild:
         torch.cuda.synchronize()
@@ -236,8 +236,6 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip plain/served/roofline/cpu legs")
     ap.add_argument("--profile-box", type=int, default=0, help="profiling leg: one cubic box of this many particles")
     ap.add_argument("--shape", type=int, default=0, help="profiling leg: pinned density shape (4, 6, 8)")
-    ap.add_argument("--force-shape", type=int, default=0,
-                    help="profiling leg: pinned force shape (32: one pair chain per lane, 64: two)")
     ap.add_argument("--rebuild", action="store_true", help="profiling leg: one forced rebuild in the range rb")
     ap.add_argument("--exact", action="store_true", help="profiling leg: FP64 bit-exact pair gaussian (rng exact)")
     args = ap.parse_args()
@@ -299,7 +297,7 @@ def main():
                        "parallelism": f"{world} GPU(s), {256 * world} boxes placed by mdpd_place "
                                       "(no data-path collective)",
                        "tuned": {"density_gathers_in_flight": shape_density,
-                                 "force_pair_chains_per_warp": shape_force}},
+                                 "force_lanes_per_warp_share": shape_force}},
             "clocks": clk.summary(), "gpu_launches": gpu_launches}
 
     if not args.no_extras:

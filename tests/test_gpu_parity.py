@@ -194,11 +194,9 @@ def assert_force_bar(f, ref, label, mask=None):
     assert np.all(err <= 1e-5 * np.maximum(mag, frms)), (err / np.maximum(mag, frms)).max()
 
 
-@pytest.mark.parametrize("chains", [1, 2])
 @pytest.mark.parametrize("exact", [False, True])
-def test_conservative_force_sigma0(exact, chains):
-    # chains: the force pass's pair chains per lane (both kernel shapes the autotuner picks from)
-    lam = mdpd_box(kT=0.0, gamma=0.0, exact=exact, extra=f"pair_modify chains {chains}")
+def test_conservative_force_sigma0(exact):
+    lam = mdpd_box(kT=0.0, gamma=0.0, exact=exact)
     lam.setup()
     n = lam.natoms()
     cnt, rows = gpu_rows(lam)
@@ -209,9 +207,8 @@ def test_conservative_force_sigma0(exact, chains):
     assert_force_bar(f[:n], ref, f"sigma=0 forces ({'exact' if exact else 'fast'} rng)")
 
 
-@pytest.mark.parametrize("chains", [1, 2])
-def test_full_force_with_exact_rng(chains):
-    lam = mdpd_box(exact=True, extra=f"pair_modify chains {chains}")
+def test_full_force_with_exact_rng():
+    lam = mdpd_box(exact=True)
     lam.setup()
     n = lam.natoms()
     cnt, rows = gpu_rows(lam)
@@ -342,12 +339,11 @@ def test_nonfinite_or_out_of_range_force_reported(A):
     assert ok.thermo().status == 0
 
 
-@pytest.mark.parametrize("chains", [1, 2])
-def test_virial_and_pair_energy_match_oracle(chains):
+def test_virial_and_pair_energy_match_oracle():
     # thermo's virial tensor and pair energy (compute pressure/meso, pe/meso) after setup,
     # against the oracle's per-atom sums over full rows (each pair twice at half weight; the
     # pair-once pass adds each pair once at full weight); exact RNG, FP32 pair terms vs FP64
-    lam = mdpd_box(exact=True, extra=f"pair_modify chains {chains}")
+    lam = mdpd_box(exact=True)
     lam.setup()
     t = lam.thermo()
     cnt, rows = gpu_rows(lam)

@@ -546,15 +546,12 @@ int mdpd_batch_time(mdpd_batch_t *b, int64_t nsteps, double *ms)
 static std::vector<StepConfig> tune_candidates(const StepConfig &base)
 {
     std::vector<StepConfig> cands;
-    if (base.half) {  // pair-once passes: the density pass's gathers in flight, the force pass's
-                      // pair chains per lane (two on single-type batches)
-        for (int slots = 1; slots <= (base.uniform_types ? 2 : 1); ++slots)
-            for (int g : {4, 6, 8}) {
-                StepConfig c = base;
-                c.gather = g;
-                c.force_slots = slots;
-                cands.push_back(c);
-            }
+    if (base.half) {  // pair-once passes: the density pass's gathers in flight
+        for (int g : {4, 6, 8}) {
+            StepConfig c = base;
+            c.gather = g;
+            cands.push_back(c);
+        }
     } else {  // full-list passes: threads per particle of each pass
         for (int td : {1, 2, 4})
             for (int tf : {1, 2, 4}) {
@@ -571,7 +568,7 @@ static TunePick pick_of(const StepConfig &c, double ms)
 {
     TunePick p;
     p.density = c.half ? c.gather : c.tpp_density;
-    p.force = c.half ? 32 * c.force_slots : c.tpp_force;
+    p.force = c.half ? 32 : c.tpp_force;
     p.ms_per_step = ms;
     return p;
 }

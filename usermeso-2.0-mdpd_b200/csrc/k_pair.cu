@@ -321,227 +321,6 @@ __device__ __forceinline__ void force_pairs(const BoxDesc &B, const Unit &U, Row
     if (EV) ev_to_partial<EV>(B, U, ev, S.red);
 }
 
-// ---------------------------------------------------------------------------------------------
-// force pass, two pair chains per lane (single-type batches)
-// ---------------------------------------------------------------------------------------------
-// The lane's share [m0, m1) of the warp's concatenated compact rows is split in two halves, each
-// walked by its own slot; every iteration evaluates one pair of each slot, so two independent
-// TEA chains and two gathers are in flight per lane, and the pair arithmetic of the two goes
-// through the two-lane FP32 instructions.  Sums, ownership and partner atomics are those of
-// force_pairs, so forces agree with it to FP32 rounding and are as deterministic.
-struct Slot2 {
-    int r, rbeg, rend;          // row within the warp; its first entry and end in the concatenation
-    float4 pi, vi;
-    float rho;
-    long long ax, ay, az;
-};
-
-__device__ __forceinline__ void slot_flush(const Slot2 &q, RowsSmem &S, int wb)
-{
-    sadd64(&S.lo[0][wb + q.r], &S.hi[0][wb + q.r], q.ax);
-    sadd64(&S.lo[1][wb + q.r], &S.hi[1][wb + q.r], q.ay);
-    sadd64(&S.lo[2][wb + q.r], &S.hi[2][wb + q.r], q.az);
-}
-
-// move the slot to the row holding entry m (m >= q.rend), flushing the row it leaves
-__device__ __forceinline__ void slot_advance(Slot2 &q, RowsSmem &S, const int *P, int wb, int m)
-{
-    slot_flush(q, S, wb);
-    q.ax = q.ay = q.az = 0;
-    do {
-        ++q.r;
-        q.rbeg = q.rend;
-        q.rend = P[q.r + 1];
-    } while (m >= q.rend);
-    q.pi = S.pi[wb + q.r];
-    q.vi = S.vi[wb + q.r];
-    q.rho = S.rho[wb + q.r];
-}
-
-__device__ __forceinline__ void slot_start(Slot2 &q, RowsSmem &S, const int *P, int wb, int m)
-{
-    q.r = row_of(P, m);
-    q.rbeg = P[q.r];
-    q.rend = P[q.r + 1];
-    q.pi = S.pi[wb + q.r];
-    q.vi = S.vi[wb + q.r];
-    q.rho = S.rho[wb + q.r];
-    q.ax = q.ay = q.az = 0;
-}
-
-template <bool EXACT, bool EV>
-__device__ __forceinline__ void force_pairs2(const BoxDesc &B, const Unit &U, RowsSmem &S)
-{
-    const int t = threadIdx.x, lane = t & 31, w = t >> 5, wb = t & ~31;
-    if (t == 0) S.coeff[0] = B.coeff[0];
-    const int i = U.begin + t;
-    const bool live = i < U.end;
-    int len = 0;
-    if (live) {
-        S.pi[t] = B.pos[i];
-        S.vi[t] = B.vel[i];
-        S.rho[t] = B.rho[i];
-        len = MDPD_IDX(B.count2[i], B.n_col2 + 1);
-    }
-    warp_prefix(len, lane, S.pre[w]);
-    for (int c = 0; c < 3; ++c) S.lo[c][t] = S.hi[c][t] = 0u;
-    __syncthreads();
-    const int *P = S.pre[w];
-    const int T = P[32];
-    const int i0 = U.begin + wb, nlocal = B.nlocal, ncol2 = B.n_col2;
-    const int m0 = (lane * T) >> 5, m1 = ((lane + 1) * T) >> 5;
-    const int na = (m1 - m0 + 1) >> 1, mb0 = m0 + na;  // slot a: [m0, mb0), slot b: [mb0, m1)
-    const float fix_max = B.fix_pair_max;
-    unsigned long long *fax = B.facc, *fay = B.facc + nlocal, *faz = B.facc + 2 * nlocal;
-    const PairCoeff cf = S.coeff[0];
-    const float dtis = B.dt_inv_sqrt;
-    // pair constants, both halves
-    const unsigned long long one2 = pk2(1.f, 1.f), m1_2 = pk2(-1.f, -1.f), mh2 = pk2(-0.5f, -0.5f);
-    const unsigned long long mic2 = pk2(-cf.inv_cut, -cf.inv_cut), micr2 = pk2(-cf.inv_cut_r, -cf.inv_cut_r);
-    const unsigned long long A2 = pk2(cf.A, cf.A), B2 = pk2(cf.B, cf.B), g2 = pk2(cf.gamma, cf.gamma);
-    const unsigned long long sd2 = pk2(cf.sigma * dtis, cf.sigma * dtis);
-    EvAcc ev = {0, 0, 0, 0, 0, 0, 0};
-    bool bad = false;
-    if (na > 0) {
-        Slot2 qa, qb;
-        slot_start(qa, S, P, wb, m0);
-        const bool has_b = mb0 < m1;
-        slot_start(qb, S, P, wb, has_b ? mb0 : m0);
-        for (int k = 0; k < na; ++k) {
-            const int ma = m0 + k, mb = mb0 + k;
-            const bool hb = mb < m1;
-            if (ma >= qa.rend) slot_advance(qa, S, P, wb, ma);
-            if (hb && mb >= qb.rend) slot_advance(qb, S, P, wb, mb);
-            const int ea = __ldcs(B.table2 + (size_t)(i0 + qa.r) * ncol2 + (ma - qa.rbeg));
-            const int eb = hb ? __ldcs(B.table2 + (size_t)(i0 + qb.r) * ncol2 + (mb - qb.rbeg)) : ea;
-            const int ja = MDPD_IDX(ea & kEntryIndex, n_all(B)), jb = MDPD_IDX(eb & kEntryIndex, n_all(B));
-            const float4 pja = __ldg(&B.posrho[ja]), pjb = __ldg(&B.posrho[jb]);
-            const float4 vja = __ldg(&B.vel[ja]), vjb = __ldg(&B.vel[jb]);
-            const int srca = ja < nlocal ? ja : MDPD_IDX(__ldg(&B.gsrc[ja - nlocal]), nlocal);
-            const int srcb = jb < nlocal ? jb : MDPD_IDX(__ldg(&B.gsrc[jb - nlocal]), nlocal);
-            const float4 vib = hb ? qb.vi : qa.vi;
-            const float4 pib = hb ? qb.pi : qa.pi;
-            const float rhob = hb ? qb.rho : qa.rho;
-            // geometry
-            const unsigned long long dx = sub2(pk2(qa.pi.x, pib.x), pk2(pja.x, pjb.x));
-            const unsigned long long dy = sub2(pk2(qa.pi.y, pib.y), pk2(pja.y, pjb.y));
-            const unsigned long long dz = sub2(pk2(qa.pi.z, pib.z), pk2(pja.z, pjb.z));
-            const unsigned long long rsq = dist2x2(dx, dy, dz);
-            float rsa, rsb;
-            upk2(rsq, rsa, rsb);
-            // hardware 1/sqrt refined by one Newton-Raphson step (as pair_core)
-            const unsigned long long y0 = pk2(rsqrt_ftz(rsa), rsqrt_ftz(rsb));
-            const unsigned long long ne = fma2(mul2(rsq, y0), y0, m1_2);  // -(1 - rsq y0^2)
-            const unsigned long long rinv = fma2(mul2(ne, mh2), y0, y0);
-            const unsigned long long r = mul2(rsq, rinv);
-            float ra, rb;
-            upk2(r, ra, rb);
-            const bool in_a = rsa < cf.cutsq && rsa >= 1e-20f && ra >= 1e-10f;
-            const bool in_b = hb && rsb < cf.cutsq && rsb >= 1e-20f && rb >= 1e-10f;
-            // random numbers of both pairs (TEA words of the two signatures)
-            float rna, rnb;
-            if (EXACT) {
-                rna = (float)gaussian_exact(__float_as_uint(qa.vi.w), __float_as_uint(vja.w));
-                rnb = (float)gaussian_exact(__float_as_uint(vib.w), __float_as_uint(vjb.w));
-            } else {
-                rna = gaussian_fast(__float_as_uint(qa.vi.w), __float_as_uint(vja.w));
-                rnb = gaussian_fast(__float_as_uint(vib.w), __float_as_uint(vjb.w));
-            }
-            const unsigned long long dvx = sub2(pk2(qa.vi.x, vib.x), pk2(vja.x, vjb.x));
-            const unsigned long long dvy = sub2(pk2(qa.vi.y, vib.y), pk2(vja.y, vjb.y));
-            const unsigned long long dvz = sub2(pk2(qa.vi.z, vib.z), pk2(vja.z, vjb.z));
-            const unsigned long long dot = fma2(dz, dvz, fma2(dy, dvy, mul2(dx, dvx)));
-            const unsigned long long wc = fma2(r, mic2, one2);
-            float wra, wrb;
-            upk2(fma2(r, micr2, one2), wra, wrb);
-            const unsigned long long wcr = pk2(fmaxf(wra, 0.f), fmaxf(wrb, 0.f));
-            const unsigned long long rs = add2(pk2(qa.rho, rhob), pk2(pja.w, pjb.w));
-            // (A wc + B (rho_i + rho_j) wcr) - gamma wc^2 (dr.dv)/r + sigma wc xi / sqrt(dt), over r
-            const unsigned long long cons = fma2(A2, wc, mul2(mul2(B2, rs), wcr));
-            const unsigned long long diss = mul2(mul2(mul2(mul2(g2, wc), wc), dot), rinv);
-            const unsigned long long rnd = mul2(mul2(sd2, wc), pk2(rna, rnb));
-            const unsigned long long fp = mul2(add2(sub2(cons, diss), rnd), rinv);
-            float fpa, fpb;
-            upk2(fp, fpa, fpb);
-            fpa = in_a ? fpa : 0.f;
-            fpb = in_b ? fpb : 0.f;
-            float fxa, fxb, fya, fyb, fza, fzb;
-            const unsigned long long fpp = pk2(fpa, fpb);
-            upk2(mul2(dx, fpp), fxa, fxb);
-            upk2(mul2(dy, fpp), fya, fyb);
-            upk2(mul2(dz, fpp), fza, fzb);
-            if (EV) {
-                float wca, wcb, rsa_, rsb_, dxa, dxb, dya, dyb, dza, dzb;
-                upk2(wc, wca, wcb);
-                upk2(rs, rsa_, rsb_);
-                upk2(dx, dxa, dxb);
-                upk2(dy, dya, dyb);
-                upk2(dz, dza, dzb);
-                const float wcra = fmaxf(wra, 0.f), wcrb = fmaxf(wrb, 0.f);
-                if (in_a) {
-                    ev.pe += cf.e_cut * wca * wca + cf.e_cut_r * rsa_ * wcra * wcra;
-                    ev.vxx += dxa * dxa * fpa, ev.vyy += dya * dya * fpa, ev.vzz += dza * dza * fpa;
-                    ev.vxy += dxa * dya * fpa, ev.vxz += dxa * dza * fpa, ev.vyz += dya * dza * fpa;
-                }
-                if (in_b) {
-                    ev.pe += cf.e_cut * wcb * wcb + cf.e_cut_r * rsb_ * wcrb * wcrb;
-                    ev.vxx += dxb * dxb * fpb, ev.vyy += dyb * dyb * fpb, ev.vzz += dzb * dzb * fpb;
-                    ev.vxy += dxb * dyb * fpb, ev.vxz += dxb * dzb * fpb, ev.vyz += dyb * dzb * fpb;
-                }
-            }
-            bad |= !(fabsf(fxa) < fix_max && fabsf(fya) < fix_max && fabsf(fza) < fix_max);
-            bad |= !(fabsf(fxb) < fix_max && fabsf(fyb) < fix_max && fabsf(fzb) < fix_max);
-            const long long qxa = to_fix(fxa), qya = to_fix(fya), qza = to_fix(fza);
-            const long long qxb = to_fix(fxb), qyb = to_fix(fyb), qzb = to_fix(fzb);
-            qa.ax += qxa, qa.ay += qya, qa.az += qza;
-            qb.ax += qxb, qb.ay += qyb, qb.az += qzb;  // zero when slot b is idle
-            const int da = srca - U.begin;
-            if ((unsigned)da < 128u) {
-                sadd64(&S.lo[0][da], &S.hi[0][da], -qxa);
-                sadd64(&S.lo[1][da], &S.hi[1][da], -qya);
-                sadd64(&S.lo[2][da], &S.hi[2][da], -qza);
-            } else {
-                atomicAdd(fax + srca, (unsigned long long)(-qxa));
-                atomicAdd(fay + srca, (unsigned long long)(-qya));
-                atomicAdd(faz + srca, (unsigned long long)(-qza));
-            }
-            if (hb) {
-                const int db = srcb - U.begin;
-                if ((unsigned)db < 128u) {
-                    sadd64(&S.lo[0][db], &S.hi[0][db], -qxb);
-                    sadd64(&S.lo[1][db], &S.hi[1][db], -qyb);
-                    sadd64(&S.lo[2][db], &S.hi[2][db], -qzb);
-                } else {
-                    atomicAdd(fax + srcb, (unsigned long long)(-qxb));
-                    atomicAdd(fay + srcb, (unsigned long long)(-qyb));
-                    atomicAdd(faz + srcb, (unsigned long long)(-qzb));
-                }
-            }
-        }
-        slot_flush(qa, S, wb);
-        if (has_b) slot_flush(qb, S, wb);
-    }
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&B.st->status, kErrNonFinite);
-    __syncthreads();
-    if (live) {
-        atomicAdd(fax + i, join64(S.lo[0][t], S.hi[0][t]));
-        atomicAdd(fay + i, join64(S.lo[1][t], S.hi[1][t]));
-        atomicAdd(faz + i, join64(S.lo[2][t], S.hi[2][t]));
-    }
-    if (EV) ev_to_partial<EV>(B, U, ev, S.red);
-}
-
-template <bool EXACT, bool EV>
-__global__ void __launch_bounds__(128, 6) k_force_pairs2(const BoxDesc *__restrict__ boxes,
-                                                         const Unit *__restrict__ units, int nunits)
-{
-    __shared__ RowsSmem S;
-    const int u = blockIdx.x;
-    if (u >= nunits) return;
-    const Unit U = units[u];
-    force_pairs2<EXACT, EV>(boxes[U.box], U, S);
-}
-
 // 7 blocks per SM (up to 72 registers, no spill) measured fastest against 6 and 8
 template <bool EXACT, bool EV, bool UNI>
 __global__ void __launch_bounds__(128, 7) k_force_pairs(const BoxDesc *__restrict__ boxes,
@@ -616,15 +395,7 @@ void launch_force_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, cons
 {
     const int g = u.local.n;
     if (g <= 0) return;
-    if (c.force_slots == 2 && c.uniform_types) {
-        if (c.exact_rng) {
-            if (ev) k_force_pairs2<true, true><<<g, 128, 0, s>>>(boxes, u.local.d, g);
-            else k_force_pairs2<true, false><<<g, 128, 0, s>>>(boxes, u.local.d, g);
-        } else {
-            if (ev) k_force_pairs2<false, true><<<g, 128, 0, s>>>(boxes, u.local.d, g);
-            else k_force_pairs2<false, false><<<g, 128, 0, s>>>(boxes, u.local.d, g);
-        }
-    } else if (c.exact_rng) {
+    if (c.exact_rng) {
         if (ev) force_half<true, true, false>(s, boxes, u);
         else if (c.uniform_types) force_half<true, false, true>(s, boxes, u);
         else force_half<true, false, false>(s, boxes, u);

@@ -36,8 +36,6 @@ struct StepConfig {
     int half = 0;          // mdpd without wall coupling: each pair evaluated once (k_pair.cu)
     int half_enabled = 1;  // allow the half-list passes (set per batch from the boxes)
     int gather = 6;        // pair-once density pass: neighbour positions in flight per lane (4, 6, 8)
-    int force_slots = 1;   // pair-once force pass: independent pair chains per lane (1, or 2 on
-                           // single-type batches)
     int aboundary = 0;     // fix aboundary/meso at the end of each step
     int sms = 148;
 };

@@ -666,18 +666,13 @@ void Script::command(const std::string &raw)
         dirty_ = true;
     } else if (c == "pair_modify") {
         // extensions: pair_modify rng exact|fast (FP64 bit-exact gaussian or FP32 transform);
-        // gather 4|6|8 and chains 1|2 pin the pair-once passes' shapes (the density pass's
-        // neighbour gathers in flight per lane, the force pass's pair chains per lane)
+        // gather 4|6|8 pins the pair-once density pass's neighbour gathers in flight per lane
         for (int k = 1; k + 1 <= narg; k += 2) {
             if (a[k] == "rng") spec_.exact_rng = a[k + 1] == "exact";
             else if (a[k] == "gather") {
                 const int g = inum(a[k + 1]);
                 if (g != 4 && g != 6 && g != 8) parse_error("pair_modify gather must be 4, 6 or 8");
                 cfg.gather = g;
-            } else if (a[k] == "chains") {
-                const int q = inum(a[k + 1]);
-                if (q != 1 && q != 2) parse_error("pair_modify chains must be 1 or 2");
-                cfg.force_slots = q;
             }
         }
         dirty_ = true;
