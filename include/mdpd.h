@@ -264,10 +264,11 @@ int mdpd_server_drain(mdpd_server_t *s, double timeout_s);
  * near full throughput on a B200, and a short job that arrives behind long ones is done in its own
  * time.  No counterpart in the reference (one LAMMPS run per rank group, src/main.cpp:49-117). */
 int mdpd_server_set_step_particles(mdpd_server_t *s, int64_t n);
-/* where the serving loop's time went (6 doubles): host seconds creating boxes, forming batches
+/* where the serving loop's time went (8 doubles): host seconds creating boxes, forming batches
  * (work units and captured step graphs), setting up new boxes, running chunks; device seconds of
- * the chunks; number of batches formed */
-int mdpd_server_timing(mdpd_server_t *s, double *out6);
+ * the chunks; number of batches formed; host seconds waiting with no job resident, and reading
+ * states and retiring jobs after chunks */
+int mdpd_server_timing(mdpd_server_t *s, double *out8);
 /* throughput/latency summary: particle-steps/s, step p50/p99 ms, job p50/p99 s,
  * jobs done, peak resident bytes (7 doubles) */
 int mdpd_server_stats(mdpd_server_t *s, double *out7);

@@ -76,7 +76,7 @@ struct mdpd_server_s {
     double particle_steps = 0, busy_s = 0;
     // host wall seconds of the loop's parts: box creation, batch formation (units and captured
     // graphs), setup of new boxes, stepping chunks (device time of the chunks is busy_s)
-    double t_create = 0, t_form = 0, t_setup = 0, t_chunks = 0;
+    double t_create = 0, t_form = 0, t_setup = 0, t_chunks = 0, t_wait = 0, t_retire = 0;
     int64_t n_forms = 0;
     std::vector<float> all_step_ms;
     std::vector<double> job_latency_s;
@@ -161,7 +161,11 @@ void mdpd_server_s::loop()
         std::vector<std::shared_ptr<Job>> admitted;
         {
             std::unique_lock<std::mutex> lk(mu);
-            if (active.empty()) cv.wait(lk, [&] { return stop || !queue.empty(); });
+            if (active.empty()) {
+                const double tw0 = now();
+                cv.wait(lk, [&] { return stop || !queue.empty(); });
+                t_wait += now() - tw0;
+            }
             if (stop) break;
             // admission: FIFO while the next job fits the budget
             while (!queue.empty()) {
@@ -351,11 +355,14 @@ void mdpd_server_s::loop()
             for (int64_t q = 0; q < k; ++q) all_step_ms.push_back(ms / k);
         }
         // retire finished / failed / cancelled / preempted stepping jobs
+        const double tr0 = now();
         std::vector<std::shared_ptr<Job>> out;
         std::vector<Thermo> th;
+        std::vector<BoxState> states;
+        batch->read_states(states);  // every stepping box's scalars: one gather, one copy
         for (size_t q = 0; q < stepping.size(); ++q) {
             auto &j = stepping[q];
-            const BoxState bst = j->box->state();
+            const BoxState &bst = states[q];
             j->done += k;
             for (int64_t s = 0; s < k; ++s) j->step_ms.push_back(ms / k);
             const bool fail = bst.status != 0;
@@ -372,6 +379,7 @@ void mdpd_server_s::loop()
             stepping.clear();
             drop(active, out);
         }
+        t_retire += now() - tr0;
     }
     batch.reset();
     for (auto &j : active) j->box.reset();
@@ -548,6 +556,8 @@ int mdpd_server_timing(mdpd_server_t *s, double *o)
     o[3] = s->t_chunks;
     o[4] = s->busy_s;
     o[5] = (double)s->n_forms;
+    o[6] = s->t_wait;
+    o[7] = s->t_retire;
     return MDPD_OK;
 }
 

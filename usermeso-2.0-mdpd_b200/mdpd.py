@@ -451,12 +451,14 @@ class Server:
 
     def timing(self):
         """seconds in box creation, batch formation, setup of new boxes and chunks (host), the
-        chunks' device seconds, and the number of batches formed"""
-        o = np.zeros(6)
+        chunks' device seconds, the number of batches formed, and host seconds waiting with no
+        job resident and retiring jobs"""
+        o = np.zeros(8)
         rc = lib().mdpd_server_timing(self.h, _ptr(o, C.c_double))
         if rc:
             raise MdpdError(rc, "timing failed")
-        return dict(zip(["create_s", "form_s", "setup_s", "chunks_s", "busy_s", "forms"], o.tolist()))
+        return dict(zip(["create_s", "form_s", "setup_s", "chunks_s", "busy_s", "forms", "wait_s", "retire_s"],
+                        o.tolist()))
 
     def set_step_particles(self, n):
         """particles stepped together: the resident jobs with the least remaining work, up to n
