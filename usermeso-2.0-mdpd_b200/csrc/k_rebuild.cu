@@ -239,12 +239,41 @@ __device__ __forceinline__ float4 list_pos(const float4 &p, int i, int nlocal)
     return make_float4(p.x, p.y, p.z, __int_as_float(wd));
 }
 
+// One bucket's members in (key, index) order by the whole warp: the ranks from a shared-memory
+// copy of the keys (buckets of up to kClassMax members).
+template <int MODE>
+__device__ __forceinline__ void bucket_warp(const BoxDesc &B, int *arr, int s, int n, int lane,
+                                            unsigned long long *key)
+{
+    const int lim = MODE == 0 ? B.nlocal : n_all(B);
+    for (int e = lane; e < n; e += 32) {
+        const int idx = MDPD_IDX(arr[s + e], lim);
+        key[e] = MODE == 0 ? (((unsigned long long)(uint32_t)B.sub_of[idx] << 32) | (uint32_t)idx)
+                           : (unsigned long long)(uint32_t)idx;
+    }
+    __syncwarp();
+    for (int e = lane; e < n; e += 32) {
+        const unsigned long long k = key[e];
+        int rank = 0;
+        for (int q = 0; q < n; ++q) rank += key[q] < k;
+        const int idx = (int)(uint32_t)k;
+        arr[s + rank] = idx;
+        if (MODE == 1) B.bpos[s + rank] = list_pos(B.pos[idx], idx, B.nlocal);
+    }
+    __syncwarp();
+}
+
+// Buckets are taken four at a time per warp, one per group of 8 lanes: a bucket of up to 8
+// members (the usual case: a bin's locals split into two reorder classes, or a border bin) is
+// ordered with shuffles inside its group, so the warp waits once for the loads of four buckets;
+// a larger one is ordered by the whole warp afterwards.
 template <int MODE>  // 0: reorder classes -> perm, 1: bins -> bin_order + bpos
 __global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict__ boxes,
                                                    const Unit *__restrict__ units, int nunits)
 {
     __shared__ unsigned long long s_key[8][kClassMax];
     const int lane = threadIdx.x & 31, w = threadIdx.x / 32;
+    const int grp = lane >> 3, l8 = lane & 7;
     unsigned long long *key = s_key[w];
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const Unit U = units[u];
@@ -253,43 +282,61 @@ __global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict_
         int *cnt = MODE == 0 ? B.cls_count : B.bin_count;
         const int *start = MODE == 0 ? B.cls_start : B.bin_start;
         int *arr = MODE == 0 ? B.perm : B.bin_order;
-        for (int b = U.begin + w; b < U.end; b += 8) {
-            const int n = cnt[b];
-            if (n == 0) continue;
-            const int s = start[b];
-            __syncwarp();
-            if (!(MDPD_IN(s, s + n) && MDPD_IN(s + n - 1, MODE == 0 ? B.nlocal : n_all(B)))) {
-                if (lane == 0) cnt[b] = 0;  // check build: a bucket outside its array
-                continue;
+        const int lim = MODE == 0 ? B.nlocal : n_all(B);
+        for (int b0 = U.begin + 4 * w; b0 < U.end; b0 += 32) {
+            const int b = b0 + grp;
+            int n = 0, s = 0;
+            if (b < U.end) {
+                n = cnt[b];
+                s = start[b];
             }
-            if (MODE == 1 && arr[s + n - 1] < B.nlocal) {
-                // locals only: already in index order, bpos written by the scatter
-                if (lane == 0) cnt[b] = 0;
-                continue;
+            if (n != 0 && !(MDPD_IN(s, s + n) && MDPD_IN(s + n - 1, lim))) {
+                if (l8 == 0) cnt[b] = 0;  // check build: a bucket outside its array
+                n = 0;
             }
-            if (n > kClassMax) {
-                if (lane == 0) {
-                    atomicOr(&B.st->status, kErrBucketOverflow);
-                    cnt[b] = 0;
-                }
-                continue;
+            const bool small = n > 0 && n <= 8;
+            const bool member = small && l8 < n;
+            int idx = 0;
+            unsigned long long k = ~0ull;
+            if (member) {
+                idx = MDPD_IDX(arr[s + l8], lim);
+                k = MODE == 0 ? (((unsigned long long)(uint32_t)B.sub_of[idx] << 32) | (uint32_t)idx)
+                              : (unsigned long long)(uint32_t)idx;
             }
-            for (int e = lane; e < n; e += 32) {
-                const int idx = MDPD_IDX(arr[s + e], MODE == 0 ? B.nlocal : n_all(B));
-                key[e] = MODE == 0 ? (((unsigned long long)(uint32_t)B.sub_of[idx] << 32) | (uint32_t)idx)
-                                   : (unsigned long long)(uint32_t)idx;
+            // bins of locals only are already in index order, bpos written by the scatter
+            bool keep_order = false;
+            if (MODE == 1) {
+                const unsigned ghosts = __ballot_sync(0xffffffffu, member && idx >= B.nlocal);
+                keep_order = ((ghosts >> (grp * 8)) & 0xFFu) == 0;
             }
-            __syncwarp();
-            for (int e = lane; e < n; e += 32) {
-                const unsigned long long k = key[e];
-                int rank = 0;
-                for (int q = 0; q < n; ++q) rank += key[q] < k;
-                const int idx = (int)(uint32_t)k;
+            int rank = 0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const unsigned long long kq = __shfl_sync(0xffffffffu, k, (grp << 3) | q);
+                rank += (q < n && kq < k) ? 1 : 0;
+            }
+            if (member && !keep_order) {
                 arr[s + rank] = idx;
                 if (MODE == 1) B.bpos[s + rank] = list_pos(B.pos[idx], idx, B.nlocal);
             }
-            __syncwarp();
-            if (lane == 0) cnt[b] = 0;
+            if (small && l8 == 0) cnt[b] = 0;
+            // buckets of more than 8 members: the whole warp, one after another
+            unsigned big = __ballot_sync(0xffffffffu, l8 == 0 && n > 8);
+            while (big) {
+                const int leader = __ffs(big) - 1;
+                big &= big - 1;
+                const int bb = b0 + (leader >> 3);
+                const int nb = __shfl_sync(0xffffffffu, n, leader), sb = __shfl_sync(0xffffffffu, s, leader);
+                __syncwarp();
+                const bool locals_only = MODE == 1 && arr[sb + nb - 1] < B.nlocal;
+                if (!locals_only) {
+                    if (nb > kClassMax) {
+                        if (lane == 0) atomicOr(&B.st->status, kErrBucketOverflow);
+                    } else
+                        bucket_warp<MODE>(B, arr, sb, nb, lane, key);
+                }
+                if (lane == 0) cnt[bb] = 0;
+            }
         }
     }
 }
