@@ -294,6 +294,10 @@ __global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict_
                 if (l8 == 0) cnt[b] = 0;  // check build: a bucket outside its array
                 n = 0;
             }
+            // a bin whose last member is a local holds locals only (they come first in a bin):
+            // it is already in index order; its test is loaded for the four bins at once
+            bool locals_only = false;
+            if (MODE == 1 && n > 8 && l8 == 0) locals_only = arr[s + n - 1] < B.nlocal;
             const bool small = n > 0 && n <= 8;
             const bool member = small && l8 < n;
             int idx = 0;
@@ -321,20 +325,18 @@ __global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict_
             }
             if (small && l8 == 0) cnt[b] = 0;
             // buckets of more than 8 members: the whole warp, one after another
-            unsigned big = __ballot_sync(0xffffffffu, l8 == 0 && n > 8);
+            if (locals_only) cnt[b] = 0;
+            unsigned big = __ballot_sync(0xffffffffu, l8 == 0 && n > 8 && !locals_only);
             while (big) {
                 const int leader = __ffs(big) - 1;
                 big &= big - 1;
                 const int bb = b0 + (leader >> 3);
                 const int nb = __shfl_sync(0xffffffffu, n, leader), sb = __shfl_sync(0xffffffffu, s, leader);
                 __syncwarp();
-                const bool locals_only = MODE == 1 && arr[sb + nb - 1] < B.nlocal;
-                if (!locals_only) {
-                    if (nb > kClassMax) {
-                        if (lane == 0) atomicOr(&B.st->status, kErrBucketOverflow);
-                    } else
-                        bucket_warp<MODE>(B, arr, sb, nb, lane, key);
-                }
+                if (nb > kClassMax) {
+                    if (lane == 0) atomicOr(&B.st->status, kErrBucketOverflow);
+                } else
+                    bucket_warp<MODE>(B, arr, sb, nb, lane, key);
                 if (lane == 0) cnt[bb] = 0;
             }
         }
