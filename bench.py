@@ -304,7 +304,6 @@ def main():
         # ---- e2e through the C ABI on every rank (its own box set): pinned host arrays in,
         # every step's thermo read back, final state into pinned host arrays; creation, upload
         # and setup inside the timing; particle-steps summed, wall time max over ranks ----
-        import ctypes
         xs = [x for x, _ in eq_states]
         vs = [v for _, v in eq_states]
 
@@ -324,10 +323,10 @@ def main():
         be = mdpd.Batch(sp, device=local)
         be.setup()
         t1 = time.perf_counter()
-        temps = []
-        for _ in range(args.steps):
-            be.step(1)
-            temps.append([t.temp for t in be.thermo_all()])  # the step's result: every box's thermo
+        # K steps; every step's result (every box's thermo, with that step's energy and virial)
+        # comes back to the host while the next step runs
+        th, thermo_bytes = be.run_thermo(args.steps)
+        temps = [[t.temp for t in row] for row in th]
         t2 = time.perf_counter()
         for k in range(len(cfg)):
             be.state(k, xout[k], vout[k])
@@ -337,13 +336,14 @@ def main():
         state_bytes = 48 * ntot
         e2e_value, e2e_max_s = aggregate(ntot * args.steps, e2e_s, world)
         all_state_bytes, _ = aggregate(state_bytes, 1.0, world)  # summed over ranks
+        all_thermo_bytes, _ = aggregate(thermo_bytes, 1.0, world)
         line["e2e"] = {"value": e2e_value, "unit": "particle-steps/s",
                        "h2d_bytes_per_step": int(all_state_bytes / args.steps),
-                       "d2h_bytes_per_step": int(all_state_bytes / args.steps +
-                                                 world * len(cfg) * ctypes.sizeof(mdpd.Thermo)),
+                       "d2h_bytes_per_step": int(all_state_bytes / args.steps + all_thermo_bytes),
                        "note": "wall clock of: create of all 256 boxes from pinned host x, v; setup; K steps, "
-                               "each followed by a read of every box's thermo; full state download into "
-                               "pinned host arrays",
+                               "each followed by a read of every box's thermo (mdpd_batch_run_thermo: step k's "
+                               "thermo comes back while step k+1 runs); full state download into pinned host "
+                               "arrays",
                        "split": split}
         del temps, xin, vin, xout, vout
 

@@ -152,6 +152,14 @@ int mdpd_batch_thermo(mdpd_batch_t *b, int32_t box, mdpd_thermo_t *out);
  * compute_pressure_meso.cu:98-150) that mdpd_batch_thermo returns one at a time */
 int mdpd_batch_thermo_all(mdpd_batch_t *b, mdpd_thermo_t *out, int32_t nbox);
 int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int64_t n);
+/* nsteps steps of every box, each step's thermo (every box, with that step's energy and virial:
+ * a LAMMPS thermo line at every step, Run::command with thermo 1) written to
+ * out[k * nbox + box], k = 0 .. nsteps-1.  Step k's thermo comes back to the host while step k+1
+ * runs, through pinned staging the batch keeps, so the readback costs no device idle time.
+ * *d2h_bytes_per_step (optional): device-to-host bytes copied per step.  A box's device error
+ * bits seen in any step's thermo make the call return MDPD_ERR_NAN / MDPD_ERR_OVERFLOW after all
+ * nsteps (the records still hold every step). */
+int mdpd_batch_run_thermo(mdpd_batch_t *b, int64_t nsteps, mdpd_thermo_t *out, int64_t *d2h_bytes_per_step);
 /* project autotuner: times the candidate shapes of the pair passes on this batch (13 real steps
  * each, so the boxes advance) and keeps the fastest. Pair-once mDPD batches: *shape_density =
  * neighbour gathers in flight per lane in the density pass (4, 6 or 8), *shape_force = 32 (a

@@ -56,6 +56,30 @@ def test_batch_equals_alone_bitwise(gather):
     b.close()
 
 
+def test_run_thermo_reads_every_step_as_step_and_thermo_do():
+    # the pipelined call (step k's thermo read back while step k+1 runs) gives, for every step and
+    # box, exactly what a step followed by a synchronous thermo read gives
+    sp = specs()
+    a = mdpd.Batch(sp)
+    a.setup()
+    ref = []
+    for _ in range(12):
+        a.step(1)
+        ref.append([(t.step, t.temp, t.pe, t.press, t.nbuild) for t in a.thermo_all()])
+    xa = [a.state(k) for k in range(len(sp))]
+    a.close()
+    b = mdpd.Batch(sp)
+    b.setup()
+    th, nbytes = b.run_thermo(12)
+    assert nbytes > 0
+    got = [[(t.step, t.temp, t.pe, t.press, t.nbuild) for t in row] for row in th]
+    assert got == ref
+    for k in range(len(sp)):
+        xb, vb = b.state(k)
+        assert np.array_equal(xa[k][0], xb) and np.array_equal(xa[k][1], vb)
+    b.close()
+
+
 def test_server_continuous_batching_matches_alone():
     sp = specs()
     steps = [90, 150, 60, 120]

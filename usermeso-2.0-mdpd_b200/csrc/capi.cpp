@@ -481,6 +481,23 @@ int mdpd_batch_step(mdpd_batch_t *b, int64_t nsteps)
     });
 }
 
+int mdpd_batch_run_thermo(mdpd_batch_t *b, int64_t nsteps, mdpd_thermo_t *out, int64_t *d2h_bytes_per_step)
+{
+    if (!b || nsteps < 0 || (nsteps > 0 && !out)) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        const size_t nb = b->boxes.size();
+        int bad = 0;
+        b->batch->run_thermo(nsteps, [&](long long k, const std::vector<Thermo> &t) {
+            for (size_t q = 0; q < nb; ++q) {
+                fill_thermo(t[q], out + (size_t)k * nb + q);
+                bad |= t[q].status;
+            }
+        });
+        if (d2h_bytes_per_step) *d2h_bytes_per_step = (int64_t)b->batch->thermo_bytes_per_step();
+        if (bad) throw ScriptError(bad & kErrNonFinite ? MDPD_ERR_NAN : MDPD_ERR_OVERFLOW, status_text(bad));
+    });
+}
+
 int mdpd_batch_thermo(mdpd_batch_t *b, int32_t box, mdpd_thermo_t *out)
 {
     if (!b || !out || box < 0 || box >= (int)b->boxes.size()) return MDPD_ERR_ARG;

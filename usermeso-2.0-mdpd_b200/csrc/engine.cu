@@ -2,6 +2,8 @@
 // IF(rebuild){...} -> density -> force), setup and thermo.
 #include "engine.h"
 
+#include <functional>
+
 #include <mutex>
 
 #include <algorithm>
@@ -530,6 +532,9 @@ Batch::~Batch()
     }
     for (Unit *u : unit_allocs_) cudaFree(u);
     cudaFree(d_boxes);
+    if (h_stage_) cudaFreeHost(h_stage_);
+    for (auto &e : ev_stage_)
+        if (e) cudaEventDestroy(e);
     cudaFree(d_done);
     cudaFree(d_thermo);
     cudaFree(d_states);
@@ -751,6 +756,13 @@ void Batch::thermo(std::vector<Thermo> &out)
     check_cuda(cudaStreamSynchronize(stream_), "thermo");
     std::vector<BoxState> sts;
     read_states(sts);
+    to_thermo(h.data(), sts.data(), out);
+}
+
+// every box's thermo from its reduced partials (kPartialStride doubles per box) and its scalars
+void Batch::to_thermo(const double *h, const BoxState *sts, std::vector<Thermo> &out) const
+{
+    const int nb = (int)boxes_.size();
     out.resize(nb);
     for (int b = 0; b < nb; ++b) {
         const Box &bx = *boxes_[b];
@@ -777,6 +789,45 @@ void Batch::thermo(std::vector<Thermo> &out)
         for (int k = 0; k < 6; ++k) t.ptensor[k] = (t.ke_tensor[k] + t.virial[k]) / vol;
         t.surface_tension = 0.5 * bx.desc.prd[0] * (t.ptensor[0] - 0.5 * (t.ptensor[1] + t.ptensor[2]));
     }
+}
+
+void Batch::run_thermo(long long nsteps, const std::function<void(long long, const std::vector<Thermo> &)> &sink)
+{
+    Range r("mdpd::run_thermo");
+    const int nb = (int)boxes_.size();
+    const size_t part_bytes = sizeof(double) * kPartialStride * nb, st_bytes = sizeof(BoxState) * nb;
+    if (!h_stage_) {
+        check_cuda(cudaHostAlloc(&h_stage_, 2 * (part_bytes + st_bytes), cudaHostAllocDefault), "thermo staging");
+        for (auto &e : ev_stage_) check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    }
+    auto part = [&](int slot) { return reinterpret_cast<double *>(h_stage_ + slot * (part_bytes + st_bytes)); };
+    auto states = [&](int slot) {
+        return reinterpret_cast<BoxState *>(h_stage_ + slot * (part_bytes + st_bytes) + part_bytes);
+    };
+    std::vector<Thermo> t;
+    for (long long k = 0; k <= nsteps; ++k) {
+        if (k < nsteps) {  // step k and its thermo, queued
+            const int slot = (int)(k & 1);
+            check_cuda(cudaGraphLaunch(graph_[1], stream_), "graph launch");
+            launch_thermo(stream_, d_boxes, units, d_thermo, d_done + 2);
+            launch_gather_states(stream_, d_boxes, nb, d_states);
+            check_cuda(cudaGetLastError(), "thermo launch");
+            check_cuda(cudaMemcpyAsync(part(slot), d_thermo, part_bytes, cudaMemcpyDeviceToHost, stream_), "thermo");
+            check_cuda(cudaMemcpyAsync(states(slot), d_states, st_bytes, cudaMemcpyDeviceToHost, stream_), "states");
+            check_cuda(cudaEventRecord(ev_stage_[slot], stream_), "event");
+        }
+        if (k >= 1) {  // step k - 1's results, while step k runs
+            const int slot = (int)((k - 1) & 1);
+            check_cuda(cudaEventSynchronize(ev_stage_[slot]), "thermo");
+            to_thermo(part(slot), states(slot), t);
+            sink(k - 1, t);
+        }
+    }
+}
+
+size_t Batch::thermo_bytes_per_step() const
+{
+    return (sizeof(double) * kPartialStride + sizeof(BoxState)) * boxes_.size();
 }
 
 void Batch::read_states(std::vector<BoxState> &out)

@@ -2,6 +2,8 @@
 // boxes stepped by one captured CUDA graph per step, thermo reductions.
 #pragma once
 
+#include <functional>
+
 #include <nvtx3/nvToolsExt.h>
 #include <cstdint>
 #include <string>
@@ -139,6 +141,10 @@ public:
     void profile(long long nsteps, double out[5]);
     long long rebuild_steps();             // steps whose rebuild body ran (device counter)
     void thermo(std::vector<Thermo> &out); // reduce + download (synchronous)
+    // nsteps steps, each with energy and virial and followed by its thermo; sink(k, thermo) gets
+    // step k's every-box thermo while step k + 1 runs (pinned double-buffered staging)
+    void run_thermo(long long nsteps, const std::function<void(long long, const std::vector<Thermo> &)> &sink);
+    size_t thermo_bytes_per_step() const;  // device-to-host bytes run_thermo copies per step
     int status(std::string &msg);          // OR of box status words
     void read_states(std::vector<BoxState> &out);  // every box's device scalars, one copy
     cudaStream_t stream() const { return stream_; }
@@ -156,6 +162,9 @@ private:
     std::vector<Unit *> unit_allocs_;
     cudaGraphExec_t graph_[2] = {nullptr, nullptr};  // [ev]
     cudaGraph_t graph_src_[2] = {nullptr, nullptr};
+    char *h_stage_ = nullptr;                    // run_thermo's pinned staging, two slots
+    cudaEvent_t ev_stage_[2] = {nullptr, nullptr};
+    void to_thermo(const double *partials, const BoxState *states, std::vector<Thermo> &out) const;
     void build_units();
     void capture(int ev);
 };

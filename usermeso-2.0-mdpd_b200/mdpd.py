@@ -105,6 +105,7 @@ def lib():
             "mdpd_server_cancel": ([vp, i64], C.c_int),
             "mdpd_server_drain": ([vp, C.c_double], C.c_int),
             "mdpd_server_stats": ([vp, dp], C.c_int),
+            "mdpd_batch_run_thermo": ([vp, i64, C.POINTER(Thermo), C.POINTER(i64)], C.c_int),
             "mdpd_server_set_step_particles": ([vp, C.c_int64], C.c_int),
             "mdpd_server_timing": ([vp, dp], C.c_int),
             "mdpd_server_stop": ([vp], None),
@@ -380,6 +381,14 @@ class Batch:
         t = Thermo()
         self._check(lib().mdpd_batch_thermo(self.h, box, C.byref(t)))
         return t
+
+    def run_thermo(self, nsteps):
+        """nsteps steps, every step's thermo of every box ((nsteps, nbox) array of Thermo), read
+        back while the next step runs; also the device-to-host bytes per step"""
+        t = (Thermo * (int(nsteps) * len(self.n)))()
+        nb = C.c_int64()
+        self._check(lib().mdpd_batch_run_thermo(self.h, int(nsteps), t, C.byref(nb)))
+        return [[t[k * len(self.n) + q] for q in range(len(self.n))] for k in range(int(nsteps))], nb.value
 
     def thermo_all(self):
         """every box's Thermo, batch order, from one pass"""
