@@ -142,6 +142,17 @@ size_t reserve_box_pool(size_t bytes)
     return got;
 }
 
+// a batch's own small arrays (box table, work units, counters) come from the box pool on the
+// batch's stream and go back to it stream-ordered: cudaMalloc/cudaFree here took up to ~1 s per
+// batch on a device whose pool holds a large mapped budget, which a server forming a batch for
+// each change of its stepping set paid every time
+template <class T> static T *batch_alloc(size_t count, cudaStream_t s)
+{
+    void *p = nullptr;
+    check_cuda(cudaMallocFromPoolAsync(&p, sizeof(T) * std::max<size_t>(count, 1), box_pool(), s), "batch arrays");
+    return static_cast<T *>(p);
+}
+
 template <class T> T *Box::alloc(size_t count)
 {
     const size_t bytes_ = (std::max<size_t>(count, 1) * sizeof(T) + 255) & ~size_t(255);
@@ -429,7 +440,7 @@ void Box::download_by_tag(double *x, double *v, double *scratch) const
     const BoxState st = state();
     const int c = st.cur;
     double *d = scratch;
-    if (!d) check_cuda(cudaMalloc(&d, sizeof(double) * 6 * (size_t)n), "download");
+    if (!d) d = batch_alloc<double>(6 * (size_t)n, 0);  // the box pool, stream-ordered
     launch_gather_by_tag(0, desc.x[c][0], desc.x[c][1], desc.x[c][2], desc.v[c][0], desc.v[c][1], desc.v[c][2],
                          desc.tag[c], n, d, d + 3 * (size_t)n);
     check_cuda(cudaGetLastError(), "download");
@@ -437,7 +448,7 @@ void Box::download_by_tag(double *x, double *v, double *scratch) const
     if (v) check_cuda(cudaMemcpyAsync(v, d + 3 * (size_t)n, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, 0),
                       "download");
     check_cuda(cudaStreamSynchronize(0), "download");
-    if (!scratch) cudaFree(d);
+    if (!scratch) cudaFreeAsync(d, 0);
 }
 
 BoxState Box::state() const
@@ -506,7 +517,7 @@ Batch::Batch(std::vector<Box *> boxes, const StepConfig &c) : cfg(c), boxes_(std
     cfg.half = cfg.style == 0 && !cfg.wall_coupling && cfg.half_enabled;
     check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
     const int nb = (int)boxes_.size();
-    check_cuda(cudaMalloc(&d_boxes, sizeof(BoxDesc) * nb), "boxes");
+    d_boxes = batch_alloc<BoxDesc>(nb, stream_);
     std::vector<BoxDesc> h(nb);
     for (int b = 0; b < nb; ++b) {
         h[b] = boxes_[b]->desc;
@@ -514,12 +525,12 @@ Batch::Batch(std::vector<Box *> boxes, const StepConfig &c) : cfg(c), boxes_(std
         h[b].list_reduce = cfg.half && !cfg.wall && !h[b].wall_fix && !h[b].ab_mobile_bit &&
                            h[b].rn2_list < h[b].rc2_tail;
     }
-    check_cuda(cudaMemcpy(d_boxes, h.data(), sizeof(BoxDesc) * nb, cudaMemcpyHostToDevice), "boxes");
-    check_cuda(cudaMalloc(&d_done, sizeof(int) * 4), "done");
-    check_cuda(cudaMemset(d_done, 0, sizeof(int) * 4), "done");
-    check_cuda(cudaMalloc(&d_thermo, sizeof(double) * kPartialStride * nb), "thermo");
-    check_cuda(cudaMalloc(&d_states, sizeof(BoxState) * nb), "states");
-    build_units();
+    check_cuda(cudaMemcpyAsync(d_boxes, h.data(), sizeof(BoxDesc) * nb, cudaMemcpyHostToDevice, stream_), "boxes");
+    d_done = batch_alloc<int>(4, stream_);
+    check_cuda(cudaMemsetAsync(d_done, 0, sizeof(int) * 4, stream_), "done");
+    d_thermo = batch_alloc<double>((size_t)kPartialStride * nb, stream_);
+    d_states = batch_alloc<BoxState>(nb, stream_);
+    build_units();  // synchronises the stream: h, the units and the counters are in place
     capture(0);
     capture(1);
 }
@@ -530,20 +541,20 @@ Batch::~Batch()
         if (graph_[k]) cudaGraphExecDestroy(graph_[k]);
         if (graph_src_[k]) cudaGraphDestroy(graph_src_[k]);
     }
-    for (Unit *u : unit_allocs_) cudaFree(u);
-    cudaFree(d_boxes);
+    // stream-ordered: after every kernel this batch queued; the stream is released once its
+    // work is done
+    for (Unit *u : unit_allocs_) cudaFreeAsync(u, stream_);
+    for (void *p : {(void *)d_boxes, (void *)d_done, (void *)d_thermo, (void *)d_states})
+        if (p) cudaFreeAsync(p, stream_);
     if (h_stage_) cudaFreeHost(h_stage_);
     for (auto &e : ev_stage_)
         if (e) cudaEventDestroy(e);
-    cudaFree(d_done);
-    cudaFree(d_thermo);
-    cudaFree(d_states);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
 // units of the boxes `which` (indices into the batch); device arrays appended to allocs
 static BatchUnits make_units(const std::vector<Box *> &boxes, const std::vector<int> &which, int nbox,
-                             std::vector<Unit *> &allocs)
+                             std::vector<Unit *> &allocs, cudaStream_t s)
 {
     std::vector<Unit> loc, all, cls, bins, scls, sgh, sbin;
     for (int b : which) {
@@ -560,9 +571,9 @@ static BatchUnits make_units(const std::vector<Box *> &boxes, const std::vector<
         chunk(sbin, B.nbin, kScanChunk);
     }
     auto up = [&](const std::vector<Unit> &v) {
-        Unit *d = nullptr;
-        check_cuda(cudaMalloc(&d, sizeof(Unit) * std::max<size_t>(v.size(), 1)), "units");
-        check_cuda(cudaMemcpy(d, v.data(), sizeof(Unit) * v.size(), cudaMemcpyHostToDevice), "units");
+        Unit *d = batch_alloc<Unit>(v.size(), s);
+        if (!v.empty())
+            check_cuda(cudaMemcpyAsync(d, v.data(), sizeof(Unit) * v.size(), cudaMemcpyHostToDevice, s), "units");
         allocs.push_back(d);
         return UnitList{d, (int)v.size()};
     };
@@ -575,6 +586,7 @@ static BatchUnits make_units(const std::vector<Box *> &boxes, const std::vector<
     u.scan_ghost = up(sgh);
     u.scan_bin = up(sbin);
     u.nbox = nbox;  // box-indexed kernels (scan tops, build counters) see every box of the batch
+    check_cuda(cudaStreamSynchronize(s), "units");  // the host vectors above are the copies' sources
     return u;
 }
 
@@ -582,7 +594,7 @@ void Batch::build_units()
 {
     std::vector<int> every(boxes_.size());
     for (size_t b = 0; b < boxes_.size(); ++b) every[b] = (int)b;
-    units = make_units(boxes_, every, (int)boxes_.size(), unit_allocs_);
+    units = make_units(boxes_, every, (int)boxes_.size(), unit_allocs_, stream_);
 }
 
 void Batch::capture(int ev)
@@ -651,22 +663,21 @@ void Batch::setup_boxes(const std::vector<int> &which)
 {
     Range r("mdpd::setup");
     if (which.empty()) return;
-    int *d = nullptr;
-    check_cuda(cudaMallocAsync(&d, sizeof(int) * which.size(), stream_), "setup boxes");
+    int *d = batch_alloc<int>(which.size(), stream_);
     check_cuda(cudaMemcpyAsync(d, which.data(), sizeof(int) * which.size(), cudaMemcpyHostToDevice, stream_),
                "setup boxes");
     k_set_rebuild<<<1, 256, 0, stream_>>>(d_boxes, d, (int)which.size(), units.nbox);
     // the passes visit the new boxes only (the others keep their state and forces)
     std::vector<Unit *> allocs;
-    const BatchUnits su = make_units(boxes_, which, units.nbox, allocs);
+    const BatchUnits su = make_units(boxes_, which, units.nbox, allocs, stream_);
     launch_rebuild(stream_, d_boxes, su, cfg, d_done);
     if (cfg.style == 0) launch_density(stream_, d_boxes, su, cfg);
     launch_force(stream_, d_boxes, su, cfg, 1, 0);
     launch_force_rebuild_flag(stream_, d_boxes, units.nbox, 0);
     check_cuda(cudaFreeAsync(d, stream_), "setup boxes");
+    for (Unit *a : allocs) cudaFreeAsync(a, stream_);
     check_cuda(cudaGetLastError(), "setup launch");
     check_cuda(cudaStreamSynchronize(stream_), "setup");
-    for (Unit *a : allocs) cudaFree(a);
 }
 
 void Batch::reconfigure(const StepConfig &c)
