@@ -378,8 +378,27 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
         }
         arena_ = static_cast<char *>(a);
     }
-    check_cuda(cudaMemsetAsync(arena_, 0, arena_need_, 0), "memset");
     layout(s, na);  // hand out the pieces
+    {
+        // zero everything but the neighbour tables (most of the arena): every build writes each
+        // list entry it later reads, and each density pass each compact entry
+        auto zero = [&](const void *from, const void *to) {
+            const char *a = static_cast<const char *>(from), *b = static_cast<const char *>(to);
+            if (b > a) check_cuda(cudaMemsetAsync(const_cast<char *>(a), 0, (size_t)(b - a), 0), "memset");
+        };
+        const char *end = arena_ + arena_need_;
+        const char *t1 = reinterpret_cast<const char *>(desc.table), *t1e = t1 + sizeof(int) * (size_t)desc.nrow * desc.n_col;
+        if (desc.table2) {
+            const char *t2 = reinterpret_cast<const char *>(desc.table2);
+            const char *t2e = t2 + sizeof(int) * (size_t)desc.nrow * desc.n_col2;
+            zero(arena_, t1);
+            zero(t1e, t2);
+            zero(t2e, end);
+        } else {
+            zero(arena_, t1);
+            zero(t1e, end);
+        }
+    }
     if (s.step0 != 0) {  // a restarted box: its step counter continues (after the memset, same stream)
         BoxState st{};
         st.step = s.step0;
@@ -819,8 +838,8 @@ void Batch::run_thermo(long long nsteps, const std::function<void(long long, con
     for (long long k = 0; k <= nsteps; ++k) {
         if (k < nsteps) {  // step k and its thermo, queued
             const int slot = (int)(k & 1);
+            // the step graph with energy and virial ends with the thermo reduction into d_thermo
             check_cuda(cudaGraphLaunch(graph_[1], stream_), "graph launch");
-            launch_thermo(stream_, d_boxes, units, d_thermo, d_done + 2);
             launch_gather_states(stream_, d_boxes, nb, d_states);
             check_cuda(cudaGetLastError(), "thermo launch");
             check_cuda(cudaMemcpyAsync(part(slot), d_thermo, part_bytes, cudaMemcpyDeviceToHost, stream_), "thermo");
