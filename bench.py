@@ -371,6 +371,7 @@ def main():
         b4 = mdpd.Batch([s4], device=local)
         b4.setup()
         b4.step(args.equil)
+        tuned4 = b4.tune()  # the project autotuner's shape for this box (13 untimed steps per candidate)
         b4.step(args.warmup)
         torch.cuda.nvtx.range_push("pair_profile")  # ncu --nvtx-include pair_profile/: the launch list
         prof = b4.profile(max(10, args.steps // 2))
@@ -389,7 +390,8 @@ def main():
                             "density_ms": prof["density_ms"], "force_ms": prof["force_ms"],
                             "density_frac": B_RHO * n4 / (prof["density_ms"] / 1e3) / 1e9 / peak,
                             "force_frac": B_F * n4 / (prof["force_ms"] / 1e3) / 1e9 / peak,
-                            "integrate_ms": prof["integrate_ms"], "rebuild_ms_avg": prof["rebuild_ms"]}
+                            "integrate_ms": prof["integrate_ms"], "rebuild_ms_avg": prof["rebuild_ms"],
+                            "tuned": {"density_gathers_in_flight": tuned4[0], "force_lanes_per_warp_share": tuned4[1]}}
         line["single_box_4M"] = {"value": n4 / (ms4 / 1e3), "unit": "particle-steps/s", "ms_per_step": ms4}
 
         # ---- served: config 5 at its spec over a fixed window ----------------------------------
