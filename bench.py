@@ -41,7 +41,7 @@ WORKLOAD = ("batched mDPD: 256 periodic boxes, N log-uniform in [2k,200k], rho 6
             "A~U[-50,-30], B~U[20,30], r_d~U[0.7,0.8], kT 1, gamma 4.5, dt 0.01, skin 0.3")
 
 
-def config4(seed, nbox=256):
+def batched_boxes(seed, nbox=256):
     rng = np.random.default_rng(seed)
     n = np.exp(rng.uniform(np.log(2000), np.log(200000), nbox)).astype(int)
     A = rng.uniform(-50, -30, nbox); B = rng.uniform(20, 30, nbox); rd = rng.uniform(0.7, 0.8, nbox)
@@ -50,10 +50,10 @@ def config4(seed, nbox=256):
 
 
 def rank_boxes(rank, world):
-    """This rank's boxes of the weak-scaling workload: world x 256 config-4 boxes (seeds
+    """This rank's boxes of the weak-scaling workload: world x 256 boxes of the batched workload (seeds
     1..world), placed on the ranks by the library's mdpd_place (particles balanced under a 150 GB
     budget per GPU).  Every rank computes the same placement; nothing is exchanged."""
-    cfg = sum((config4(seed=1 + r) for r in range(world)), [])
+    cfg = sum((batched_boxes(seed=1 + r) for r in range(world)), [])
     if world == 1:
         return cfg
     import mdpd
@@ -186,7 +186,7 @@ def run_reference(args, rank, world):
     CPU mDPD style) on the host cores, same workload, bounded sample per step."""
     if rank != 0:
         return
-    cfg = config4(seed=1)
+    cfg = batched_boxes(seed=1)
     base = cpu_baseline(cfg, budget_s=max(5.0, 0.3 * (args.steps + args.warmup)))
     line = {"impl": "reference", "metric": "mDPD particle-steps/s (batched 256-box workload)",
             "value": base["value"], "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
@@ -394,9 +394,9 @@ def main():
                             "tuned": {"density_gathers_in_flight": tuned4[0], "force_lanes_per_warp_share": tuned4[1]}}
         line["single_box_4M"] = {"value": n4 / (ms4 / 1e3), "unit": "particle-steps/s", "ms_per_step": ms4}
 
-        # ---- served: config 5 at its spec over a fixed window ----------------------------------
+        # ---- served: Poisson arrivals of droplet/slab jobs over a fixed window -----------------
         # Poisson(20/s) arrivals of droplet/slab jobs for SERVE_ARRIVE_S seconds, N log-uniform in
-        # [5k, 2M], 2,000-20,000 steps each, parameters as config 4, 150 GB budget; the server
+        # [5k, 2M], 2,000-20,000 steps each, parameters as the batched workload, 150 GB budget; the server
         # runs until SERVE_WINDOW_S after the first arrival.  Throughput is the particle-steps
         # every job completed by then (finished or not) over the window's wall time.
         srv = mdpd.Server(budget_bytes=int(150e9), device=local)

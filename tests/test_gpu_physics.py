@@ -159,7 +159,7 @@ fix dn group_fluid1 density/meso along y nbin 10 every 99999 window 99998 output
 
 
 def test_gpu_temperature_agrees_with_oracle_engine():
-    # config 1 (classic DPD: 10^3 box, rho 3, a 25, gamma 4.5, sigma 3, dt 0.01): the same start
+    # the classic DPD cube (10^3 box, rho 3, a 25, gamma 4.5, sigma 3, dt 0.01): the same start
     # through the GPU path and the FP64 oracle engine; after 500 relaxation steps, 200 samples 10
     # steps apart.  The two mean temperatures agree within 1% (the spec's bar) and both sit within
     # 1% of kT.

@@ -1,4 +1,4 @@
-"""mDPD liquid-vapour slab (the config-2 geometry scaled down, and at full size): temperature, the liquid
+"""mDPD liquid-vapour slab (the 60x30x30 slab geometry scaled down, and at full size): temperature, the liquid
 density plateau and the surface tension gamma = (Lx/2)(Pxx - (Pyy+Pzz)/2), with the FP32
 random-number transform (default) against the bit-exact FP64 transform (pair_modify rng exact).
 
@@ -80,7 +80,7 @@ def test_slab_surface_tension_and_temperature():
 
 
 def slab_config2(rng_mode, seed, steps=20000, discard=2000, every=100):
-    """The config-2 slab at full size: box [-30,30]x[-15,15]x[-15,15], liquid |x| < 10 at
+    """The 60x30x30 liquid-vapour slab at full size: box [-30,30]x[-15,15]x[-15,15], liquid |x| < 10 at
     density 6.05 (108,900 particles), A=-40, B=25, r_c=1, r_d=0.75, gamma=4.5, kT=1, dt=0.01."""
     lam = mdpd.Lammps()
     lam.commands(f"""

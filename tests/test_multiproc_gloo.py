@@ -41,7 +41,7 @@ def test_two_rank_weak_scaling_reduction():
     mp.start_processes(_worker, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
     (n0, v0, t0), (n1, v1, t1) = out[0], out[1]
     import bench
-    every = sorted(c["seed"] for c in bench.config4(seed=1) + bench.config4(seed=2))
+    every = sorted(c["seed"] for c in bench.batched_boxes(seed=1) + bench.batched_boxes(seed=2))
     a, b = out["shares"]
     assert not set(a) & set(b) and sorted(a + b) == every  # each box on exactly one rank
     assert abs(n0 - n1) / (n0 + n1) < 0.01  # particles balanced between the ranks
@@ -51,7 +51,7 @@ def test_two_rank_weak_scaling_reduction():
 
 def test_box_sets_are_seeded_and_uneven():
     import bench
-    a, b = bench.config4(seed=1), bench.config4(seed=1)
+    a, b = bench.batched_boxes(seed=1), bench.batched_boxes(seed=1)
     assert a == b and len(a) == 256
     ns = [c["n"] for c in a]
     assert min(ns) >= 2000 and max(ns) <= 200000 and max(ns) / min(ns) > 20

@@ -11,7 +11,7 @@ import bench
 
 
 def specs(seed=1, nbox=256):
-    return bench.specs_of(bench.config4(seed=seed, nbox=nbox))
+    return bench.specs_of(bench.batched_boxes(seed=seed, nbox=nbox))
 
 
 def test_every_box_placed_once_and_balanced():
