@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
-def test_dpd_config1_temperature_and_momentum(tmp_path):
+def test_dpd_cube_temperature_and_momentum(tmp_path):
     # classic DPD fluid: 10^3 box, rho = 3, a = 25, gamma = 4.5, sigma = 3, dt = 0.01
     lam = mdpd.Lammps()
     lam.commands("""

@@ -79,7 +79,7 @@ def test_slab_surface_tension_and_temperature():
     assert 5.0 < top_f < 8.0
 
 
-def slab_config2(rng_mode, seed, steps=20000, discard=2000, every=100):
+def slab_full_size(rng_mode, seed, steps=20000, discard=2000, every=100):
     """The 60x30x30 liquid-vapour slab at full size: box [-30,30]x[-15,15]x[-15,15], liquid |x| < 10 at
     density 6.05 (108,900 particles), A=-40, B=25, r_c=1, r_d=0.75, gamma=4.5, kT=1, dt=0.01."""
     lam = mdpd.Lammps()
@@ -116,10 +116,10 @@ run_style mvv/meso
     return np.array(gam), np.array(tem), prof
 
 
-def test_config2_slab_full_size():
+def test_slab_60x30x30_full_size():
     # 20,000 steps, the first 2,000 discarded; block averages of 180 samples
-    gf, tf, pf = slab_config2("fast", 2024)
-    ge, te, pe = slab_config2("exact", 2024)
+    gf, tf, pf = slab_full_size("fast", 2024)
+    ge, te, pe = slab_full_size("exact", 2024)
     for t in (tf, te):  # the spec's bar at full size (the small slab above carries a ~1% bias)
         assert abs(t.mean() - 1.0) < 0.01, (tf.mean(), te.mean())
     assert abs(tf.mean() - te.mean()) < max(0.005, 3 * np.hypot(block_se(tf), block_se(te))), (tf.mean(), te.mean())
