@@ -28,6 +28,20 @@ enum { kSelCls = 0, kSelGhost = 1, kSelBin = 2 };
 
 __device__ __forceinline__ bool rebuilding(const BoxDesc &B) { return B.st->rebuild != 0; }
 
+// counter[idx] += 1 for each calling lane, one atomic per distinct idx among the converged lanes
+// (particles of one bin or class mostly sit next to each other, so a warp's lanes share few
+// counters); returns what a per-lane atomicAdd would have returned, in lane order within each idx
+__device__ __forceinline__ int warp_add1(int *counter, int idx)
+{
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, idx);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter + idx, __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + __popc(peers & ((1u << lane) - 1u));
+}
+
 // ---------------------------------------------------------------------------
 // R1: wrap + reorder key
 // ---------------------------------------------------------------------------
@@ -63,7 +77,7 @@ __global__ void __launch_bounds__(kUnit) k_rb_key(const BoxDesc *__restrict__ bo
         const int cls = MDPD_IDX((border ? B.nbin : 0) + B.bin_rank[MDPD_IDX(bin, B.nbin)], 2 * B.nbin);
         B.cls_of[i] = cls;
         B.sub_of[i] = (int)morton3(sub[0], sub[1], sub[2]);
-        atomicAdd(&B.cls_count[cls], 1);
+        warp_add1(B.cls_count, cls);
     }
 }
 
@@ -220,7 +234,7 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_cls(const BoxDesc *__restr
         if (!rebuilding(B)) continue;
         const int i = U.begin + threadIdx.x;
         if (i >= U.end) continue;
-        const int p = atomicAdd(&B.cls_cursor[MDPD_IDX(B.cls_of[i], 2 * B.nbin)], 1);
+        const int p = warp_add1(B.cls_cursor, MDPD_IDX(B.cls_of[i], 2 * B.nbin));
         B.perm[MDPD_IDX(p, B.nlocal)] = i;
     }
 }
@@ -411,7 +425,7 @@ __global__ void __launch_bounds__(kUnit) k_rb_permute(BoxDesc *__restrict__ boxe
         for (int d = 0; d < 3; ++d) bid[d] = clamp_bin(bin_coord(x[d], B.lo[d], B.bininv[d]), B.mbin[d]);
         const int bin = bid[0] + B.mbin[0] * (bid[1] + bid[2] * B.mbin[1]);
         B.bin_of[k] = bin;
-        atomicAdd(&B.bin_count[MDPD_IDX(bin, B.nbin)], 1);
+        warp_add1(B.bin_count, MDPD_IDX(bin, B.nbin));
     }
     __shared__ bool s_last;
     __syncthreads();
@@ -524,7 +538,7 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__rest
             B.bpos[p] = list_pos(B.pos[i], i, nl);
         } else {
             const int nloc = (b1 - b0) + (B.cls_start[B.nbin + rk + 1] - e0);
-            p = MDPD_IDX(atomicAdd(&B.bin_cursor[bin], 1) + nloc, n_all(B));
+            p = MDPD_IDX(warp_add1(B.bin_cursor, bin) + nloc, n_all(B));
         }
         B.bin_order[p] = i;
     }
