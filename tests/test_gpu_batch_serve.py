@@ -102,6 +102,9 @@ def test_server_continuous_batching_matches_alone():
     st = srv.stats()
     assert st["jobs_done"] == len(ids)
     assert st["peak_resident_bytes"] <= budget
+    tm = srv.timing()  # where the loop's time went: every part counted, batches were formed
+    assert all(tm[k] >= 0 for k in tm) and tm["forms"] >= 1 and tm["busy_s"] > 0
+    assert tm["chunks_s"] >= tm["busy_s"] * 0.5
     srv.stop()
 
 
