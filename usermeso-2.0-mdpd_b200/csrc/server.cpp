@@ -126,6 +126,9 @@ void mdpd_server_s::retire(Job &j, const Thermo &t, int error, bool finished)
         vf.resize(3 * (size_t)n);
         j.box->download_by_tag(xf.data(), vf.data());
     }
+    // the device memory goes back to the pool before the job is reported done, outside the lock
+    // (pollers and submitters are not held up by it)
+    j.box.reset();
     std::lock_guard<std::mutex> lk(mu);
     j.thermo = out;
     j.xf.swap(xf);
@@ -135,7 +138,6 @@ void mdpd_server_s::retire(Job &j, const Thermo &t, int error, bool finished)
     j.end_s = now();
     if (!preempted && !j.cancel) job_latency_s.push_back(j.end_s - j.submit_s);  // a preempted job goes on elsewhere
     resident -= j.bytes;
-    j.box.reset();
     cv.notify_all();
 }
 
