@@ -36,6 +36,7 @@ RC, SKIN = 1.0, 0.3
 NBAR = RHO * 4.0 / 3.0 * math.pi * (RC + SKIN) ** 3          # list entries per particle, 55.7
 B_RHO = 24 + 4 * NBAR                                         # density pass bytes / particle
 B_F = 52 + 4 * NBAR                                           # force pass bytes / particle
+B_STEP = B_RHO + B_F + 116                                    # + fused integrate (x, v, f, packs)
 SERVE_ARRIVE_S, SERVE_WINDOW_S = 10.0, 40.0  # served leg: arrival span and measured window
 WORKLOAD = ("batched mDPD: 256 periodic boxes, N log-uniform in [2k,200k], rho 6.05, "
             "A~U[-50,-30], B~U[20,30], r_d~U[0.7,0.8], kT 1, gamma 4.5, dt 0.01, skin 0.3")
@@ -392,7 +393,10 @@ def main():
                             "force_frac": B_F * n4 / (prof["force_ms"] / 1e3) / 1e9 / peak,
                             "integrate_ms": prof["integrate_ms"], "rebuild_ms_avg": prof["rebuild_ms"],
                             "tuned": {"density_gathers_in_flight": tuned4[0], "force_lanes_per_warp_share": tuned4[1]}}
-        line["single_box_4M"] = {"value": n4 / (ms4 / 1e3), "unit": "particle-steps/s", "ms_per_step": ms4}
+        line["single_box_4M"] = {"value": n4 / (ms4 / 1e3), "unit": "particle-steps/s", "ms_per_step": ms4,
+                                 "step_frac": B_STEP * n4 / (ms4 / 1e3) / 1e9 / peak,
+                                 "note": "whole graph step (rebuilds amortised) against the step's algorithmic "
+                                         "bytes, pair passes + integrate = %.1f B/particle" % B_STEP}
 
         # ---- served: Poisson arrivals of droplet/slab jobs over a fixed window -----------------
         # Poisson(20/s) arrivals of droplet/slab jobs for SERVE_ARRIVE_S seconds, N log-uniform in
