@@ -45,8 +45,9 @@ struct Job {
     std::vector<double> xf, vf;
     std::unique_ptr<Box> box;
     size_t bytes = 0;
-    bool cancel = false;
-    bool preempt = false;
+    // set by the API threads, read by the driver thread between chunks
+    std::atomic<bool> cancel{false};
+    std::atomic<bool> preempt{false};
     bool set_up = false;  // its setup (rebuild, density and force passes) has run
     double remaining() const { return (double)spec.box.n * (double)(spec.nsteps - done); }
 };
