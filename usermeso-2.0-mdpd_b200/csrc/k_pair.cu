@@ -5,11 +5,12 @@
 //   neighbour positions in flight per lane (the batch's autotuner picks G).  rho_i
 //   (fix_aboundary_rho_meso.cu:119-165) is summed in FP32 with the hardware rsqrt, as the
 //   reference forms each term; the reference adds the terms in FP64, which changes rho by about
-//   1e-7 of its mean and costs ~13 % of this pass.  The pass also writes, into the particle's row of the compact table, the entries within
-//   the force cutoff that the row owns: a local j when j > i, a ghost j when j is an image shifted
-//   in the positive direction (kUpperImage in pos.w).  The mirrored pair, seen from the other end,
-//   has the opposite shift, so every pair is owned by exactly one row.  It also writes
-//   (x, y, z, rho) of the particle and its ghost images for the force pass's gathers.
+//   1e-7 of its mean and costs ~13 % of this pass.  The pass also writes, into the particle's
+//   row of the compact table, the entries within the force cutoff that the row owns (bit 31 of
+//   the list entry, set by the list build: a local j when j > i, a ghost j when j is an image
+//   shifted in the positive direction).  The mirrored pair, seen from the other end, has the
+//   opposite shift, so every pair is owned by exactly one row.  It also writes (x, y, z, rho) of
+//   the particle and its ghost images for the force pass's gathers.
 // k_force_pairs: the 32 compact rows of a warp are concatenated and split into 32 equal
 //   contiguous shares, one per lane (a prefix scan of the row lengths and one binary search), so
 //   every lane evaluates the same number of pairs whatever the row lengths.  Each entry carries
@@ -38,8 +39,6 @@ constexpr double kFixInv = 1.0 / 4294967296.0;
 constexpr int kEntryTypeShift = 27;              // compact entry: j | (type of j - 1) << 27
 constexpr int kEntryIndex = (1 << kEntryTypeShift) - 1;
 
-__device__ __forceinline__ int nlocal_of(const BoxDesc &B) { return B.nlocal; }
-
 // ---------------------------------------------------------------------------------------------
 // density pass, global indices
 // ---------------------------------------------------------------------------------------------
@@ -53,9 +52,9 @@ __device__ __forceinline__ float rsqrt_ftz(float x)
 
 // One lane per row; the geometry of entries goes two at a time through the two-lane FP32
 // instructions.  A term is (h - r)^2 with r = rsq * rsqrt(rsq), formed as t = rsq * rsqrt(rsq) - h
-// (one rounding; t is -(h - r) exactly) and min(t, 0)^2: pairs beyond the cutoff add 0, and so do the particle's own
-// entry and coincident particles (rsq = 0 gives 0 * inf = NaN, which min() drops; a denormal rsq
-// gives inf).  The reference skips rsq < 1e-20; here a normal rsq below 1e-20 (two particles
+// (one rounding; t is -(h - r) exactly) and min(t, 0)^2: pairs beyond the cutoff add 0, and so
+// do the particle's own entry and coincident particles (rsq = 0 gives 0 * inf = NaN, which min()
+// drops; a denormal rsq gives inf).  The reference skips rsq < 1e-20; here a normal rsq below 1e-20 (two particles
 // closer than 1e-10, whose FP32 coordinates are then both below ~1e-3 in magnitude) would add
 // h^2.  Rows are padded to the warp's longest with the particle itself.  Owned entries (bit 31,
 // set by the list build) within the force cutoff go to the compact row.
@@ -129,9 +128,9 @@ template <int kGather, bool UNI> __device__ __forceinline__ void density_rows(co
         if (i >= B.st->n_bulk) {
             const int g1 = min(B.gfirst[i + 1], B.ghost_cap);
             for (int g = B.gfirst[i]; g < g1; ++g) {
-                if (in_group) B.rho[nlocal_of(B) + g] = r;
-                const float4 pg = B.pos[nlocal_of(B) + g];
-                B.posrho[nlocal_of(B) + g] = make_float4(pg.x, pg.y, pg.z, r);
+                if (in_group) B.rho[B.nlocal + g] = r;
+                const float4 pg = B.pos[B.nlocal + g];
+                B.posrho[B.nlocal + g] = make_float4(pg.x, pg.y, pg.z, r);
             }
         }
     }
