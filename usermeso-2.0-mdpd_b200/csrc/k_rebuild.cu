@@ -546,7 +546,8 @@ __global__ void __launch_bounds__(kUnit) k_rb_scatter_bins(const BoxDesc *__rest
 
 // ---------------------------------------------------------------------------
 // R11: neighbour list, warp per bin, in two phases per chunk of candidates:
-//   filter  the 27 stencil bins are streamed once (lane = candidate); a candidate is kept
+//   filter  the 27 stencil bins are streamed once (lane = candidate, its bin found from one
+//           ballot and one OR-reduction of the bins' start offsets); a candidate is kept
 //           when it lies within the cutoff of the box bounding the bin's centres (the FP32
 //           bound is exact: each axis gap rounds to at most the gap to any centre, and the
 //           squared distance is monotone in the gaps), compacted into shared memory
@@ -590,7 +591,7 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
     __shared__ float4 s_q[8][kListChunk];               // kept candidates: x, y, z, list word
     __shared__ int s_j[8][kListChunk];                  // their particle indices
     __shared__ float4 s_lo[8], s_hi[8];                 // the centres' bounding box; cmin
-    __shared__ int s_bs[8][32], s_cum[8][33];
+    __shared__ int s_d[8][32], s_ex[8][32];             // non-empty stencil bins: start - stream offset; offset
     const int lane = threadIdx.x & 31, w = threadIdx.x / 32;
     const unsigned lt = (1u << lane) - 1u;
     const int nitems = nunits * 32;
@@ -629,11 +630,20 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
             if (lane >= o) cum += v;
         }
         const int total = __shfl_sync(0xffffffffu, cum, 31);
-        s_bs[w][lane] = st;
-        s_cum[w][lane + 1] = cum;
-        if (lane == 0) s_cum[w][0] = 0;
-        int local_max = 0;
+        // the candidate stream is the non-empty stencil bins in slot order; bin k of them starts
+        // at stream offset ex_k, so stream position q is particle d_k + q of the bin order with
+        // d_k = start_k - ex_k, k the last non-empty bin with ex_k <= q
+        const unsigned ne = __ballot_sync(0xffffffffu, sz != 0);
+        if (sz != 0) {
+            const int k = __popc(ne & lt);
+            s_d[w][k] = st - (cum - sz);
+            s_ex[w][k] = cum - sz;
+        }
         __syncwarp();
+        // lane k holds ex_k of non-empty bin k (no bin: past every position)
+        const int exk = lane < __popc(ne) ? s_ex[w][lane] : 0x7fffffff;
+        const unsigned le = lt | (1u << lane);
+        int local_max = 0;
         for (int cb = s; cb < e; cb += 32) {
             // centre batch: members with index < nlocal (they come first in a bin)
             const int pc = cb + lane;
@@ -664,7 +674,6 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
                     s_hi[w] = make_float4(hix, hiy, hiz, 0.f);
                 }
             }
-            int slot = 0;  // stencil slot of this lane's stream position (only grows)
             __syncwarp();
             for (int qs = 0; qs < total;) {
                 // filter: fill up to kListChunk kept candidates
@@ -672,12 +681,15 @@ __global__ void __launch_bounds__(256, 4) k_rb_list(const BoxDesc *__restrict__ 
                 const float4 lo = s_lo[w], hi = s_hi[w];
                 for (; qs < total && nk <= kListChunk - 32; qs += 32) {
                     const int q = qs + lane;
+                    // bin of position q: the bins that start before qs, plus those that start
+                    // in [qs, q] (bit ex_k - qs of the round's start mask)
+                    const unsigned starts = __reduce_or_sync(
+                        0xffffffffu, exk >= qs && exk - qs < 32 ? 1u << (exk - qs) : 0u);
+                    const int kq = __popc(__ballot_sync(0xffffffffu, exk < qs)) + __popc(starts & le) - 1;
                     bool keep = false;
                     float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (q < total) {
-                        // largest slot with s_cum[slot] <= q (s_cum[27] = total > q ends the walk)
-                        while (s_cum[w][slot + 1] <= q) ++slot;
-                        pj = B.bpos[s_bs[w][slot] + (q - s_cum[w][slot])];
+                        pj = B.bpos[s_d[w][kq] + q];
                         const float gx = fmaxf(fmaxf(lo.x - pj.x, pj.x - hi.x), 0.f);
                         const float gy = fmaxf(fmaxf(lo.y - pj.y, pj.y - hi.y), 0.f);
                         const float gz = fmaxf(fmaxf(lo.z - pj.z, pj.z - hi.z), 0.f);
