@@ -456,12 +456,15 @@ void Box::release() noexcept
 void Box::download_by_tag(double *x, double *v, double *scratch) const
 {
     Range r("mdpd::download");
-    const BoxState st = state();
-    const int c = st.cur;
     double *d = scratch;
     if (!d) d = batch_alloc<double>(6 * (size_t)n, 0);  // the box pool, stream-ordered
-    launch_gather_by_tag(0, desc.x[c][0], desc.x[c][1], desc.x[c][2], desc.v[c][0], desc.v[c][1], desc.v[c][2],
-                         desc.tag[c], n, d, d + 3 * (size_t)n);
+    // the gather picks the live buffer on the device: one wait per call, at the end
+    StateBuffers sb;
+    for (int c = 0; c < 2; ++c) {
+        for (int k = 0; k < 3; ++k) sb.x[c][k] = desc.x[c][k], sb.v[c][k] = desc.v[c][k];
+        sb.tag[c] = desc.tag[c];
+    }
+    launch_gather_by_tag(0, sb, desc.st, n, d, d + 3 * (size_t)n);
     check_cuda(cudaGetLastError(), "download");
     if (x) check_cuda(cudaMemcpyAsync(x, d, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, 0), "download");
     if (v) check_cuda(cudaMemcpyAsync(v, d + 3 * (size_t)n, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, 0),

@@ -724,23 +724,21 @@ void launch_gather_states(cudaStream_t s, const BoxDesc *boxes, int nbox, BoxSta
     if (nbox > 0) k_gather_states<<<(nbox + 127) / 128, 128, 0, s>>>(boxes, nbox, out);
 }
 
-__global__ void k_gather_by_tag(const double *__restrict__ x0, const double *__restrict__ x1,
-                                const double *__restrict__ x2, const double *__restrict__ v0,
-                                const double *__restrict__ v1, const double *__restrict__ v2,
-                                const int *__restrict__ tag, int n, double *__restrict__ xo, double *__restrict__ vo)
+__global__ void k_gather_by_tag(StateBuffers b, const BoxState *__restrict__ st, int n, double *__restrict__ xo,
+                                double *__restrict__ vo)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int r = tag[i] - 1;
+    const int c = st->cur & 1;
+    const int r = b.tag[c][i] - 1;
     if (r < 0 || r >= n) return;  // tags are 1..n by construction
-    xo[3 * r] = x0[i], xo[3 * r + 1] = x1[i], xo[3 * r + 2] = x2[i];
-    vo[3 * r] = v0[i], vo[3 * r + 1] = v1[i], vo[3 * r + 2] = v2[i];
+    xo[3 * r] = b.x[c][0][i], xo[3 * r + 1] = b.x[c][1][i], xo[3 * r + 2] = b.x[c][2][i];
+    vo[3 * r] = b.v[c][0][i], vo[3 * r + 1] = b.v[c][1][i], vo[3 * r + 2] = b.v[c][2][i];
 }
 
-void launch_gather_by_tag(cudaStream_t s, const double *x0, const double *x1, const double *x2, const double *v0,
-                          const double *v1, const double *v2, const int *tag, int n, double *xo, double *vo)
+void launch_gather_by_tag(cudaStream_t s, const StateBuffers &b, const BoxState *st, int n, double *xo, double *vo)
 {
-    if (n > 0) k_gather_by_tag<<<(n + 255) / 256, 256, 0, s>>>(x0, x1, x2, v0, v1, v2, tag, n, xo, vo);
+    if (n > 0) k_gather_by_tag<<<(n + 255) / 256, 256, 0, s>>>(b, st, n, xo, vo);
 }
 
 void launch_thermo(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, double *out, int *)

@@ -65,9 +65,14 @@ void launch_load_state(cudaStream_t s, const double *xa, const double *va, int n
 void launch_bin_ranks(cudaStream_t s, const int mbin[3], int *rank);
 // copies of every box's BoxState into out[nbox]
 void launch_gather_states(cudaStream_t s, const BoxDesc *boxes, int nbox, BoxState *out);
-// x, v (component arrays, internal order) -> xo[3n], vo[3n] in tag order (tags 1..n)
-void launch_gather_by_tag(cudaStream_t s, const double *x0, const double *x1, const double *x2, const double *v0,
-                          const double *v1, const double *v2, const int *tag, int n, double *xo, double *vo);
+// both buffers of a box's double-buffered x, v (components) and tags
+struct StateBuffers {
+    const double *x[2][3], *v[2][3];
+    const int *tag[2];
+};
+// x, v of the live buffer (st->cur, read on the device), internal order -> xo[3n], vo[3n] in
+// tag order (tags 1..n)
+void launch_gather_by_tag(cudaStream_t s, const StateBuffers &b, const BoxState *st, int n, double *xo, double *vo);
 void launch_thermo(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, double *out, int *done);
 void launch_density_profile(cudaStream_t s, const BoxDesc *boxes, int box, const Unit *units,
                             int nunits, int dim, int groupbit, double lo, double inv, int nbin,
