@@ -553,6 +553,7 @@ Batch::Batch(std::vector<Box *> boxes, const StepConfig &c) : cfg(c), boxes_(std
     d_thermo = batch_alloc<double>((size_t)kPartialStride * nb, stream_);
     d_states = batch_alloc<BoxState>(nb, stream_);
     build_units();  // synchronises the stream: h, the units and the counters are in place
+    init_rebuild_shapes();  // occupancy queries stay out of the captures
     capture(0);
     capture(1);
 }

@@ -19,6 +19,7 @@
 //            pair-once boxes (gpu_build_neighbor_list, neigh_build_meso.cu:17-127; layout
 //            neigh_list_meso.cu:143-147)
 #include <algorithm>
+#include <mutex>
 
 #include "kernels.h"
 
@@ -779,22 +780,56 @@ void launch_bin_ranks(cudaStream_t s, const int mbin[3], int *rank)
     k_bin_ranks<<<std::min((nbin + 255) / 256, 148 * 8), 256, 0, s>>>(mbin[0], mbin[1], mbin[2], rank);
 }
 
+// Resident blocks per SM of the per-particle rebuild passes (kUnit threads each). They loop over
+// units one particle per thread, waiting on each unit's loads, so they run as fast as the SM
+// holds blocks: the grid is the occupancy the registers allow (12 to 16 blocks for the lighter
+// passes), not a fixed 8.
+struct RebuildShapes {
+    int key = 8, cls = 8, permute0 = 8, permute1 = 8, ghosts = 8, bins = 8;
+};
+static RebuildShapes g_shapes;
+static std::once_flag g_shapes_once;
+
+template <typename K> static int resident_blocks(K kernel)
+{
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kUnit, 0) != cudaSuccess || b < 1) {
+        (void)cudaGetLastError();  // a failed query leaves the fixed 8
+        return 8;
+    }
+    return b;
+}
+
+void init_rebuild_shapes()
+{
+    std::call_once(g_shapes_once, [] {
+        g_shapes.key = resident_blocks(k_rb_key);
+        g_shapes.cls = resident_blocks(k_rb_scatter_cls);
+        g_shapes.permute0 = resident_blocks(k_rb_permute<0>);
+        g_shapes.permute1 = resident_blocks(k_rb_permute<1>);
+        g_shapes.ghosts = resident_blocks(k_rb_ghosts);
+        g_shapes.bins = resident_blocks(k_rb_scatter_bins);
+    });
+}
+
 void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int *done)
 {
+    init_rebuild_shapes();  // a no-op after the first call (made before any capture)
     const int sms = c.sms;
+    const RebuildShapes &r = g_shapes;
     auto g = [&](int n, int per_sm) { return n < sms * per_sm ? (n > 0 ? n : 1) : sms * per_sm; };
-    k_rb_key<<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
+    k_rb_key<<<g(u.local.n, r.key), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
     scan<kSelCls>(s, boxes, u.scan_cls, u.nbox, sms);
-    k_rb_scatter_cls<<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
+    k_rb_scatter_cls<<<g(u.local.n, r.cls), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
     k_rb_bucket<0><<<g(u.cls.n, 5), 256, 0, s>>>(boxes, u.cls.d, u.cls.n);
     if (c.style == 0)
-        k_rb_permute<0><<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done);
+        k_rb_permute<0><<<g(u.local.n, r.permute0), kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done);
     else
-        k_rb_permute<1><<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done);
+        k_rb_permute<1><<<g(u.local.n, r.permute1), kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done);
     scan<kSelGhost>(s, boxes, u.scan_ghost, u.nbox, sms);
-    k_rb_ghosts<<<g(u.local.n, 8), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
+    k_rb_ghosts<<<g(u.local.n, r.ghosts), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
     scan<kSelBin>(s, boxes, u.scan_bin, u.nbox, sms);
-    k_rb_scatter_bins<<<g(u.all.n, 8), kUnit, 0, s>>>(boxes, u.all.d, u.all.n);
+    k_rb_scatter_bins<<<g(u.all.n, r.bins), kUnit, 0, s>>>(boxes, u.all.d, u.all.n);
     k_rb_bucket<1><<<g(u.bins.n, 5), 256, 0, s>>>(boxes, u.bins.d, u.bins.n);
     k_rb_list<<<g(u.bins.n * 32, 4), 256, 0, s>>>(boxes, u.bins.d, u.bins.n, u.nbox, done + 1);
 }

@@ -51,6 +51,8 @@ void launch_integrate(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const
 void launch_force_rebuild_flag(cudaStream_t s, BoxDesc *boxes, int nbox, int value);
 void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c,
                     int *done);
+// the rebuild passes' grid sizes from the occupancy API: call once before any stream capture
+void init_rebuild_shapes();
 void launch_density(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c);
 void launch_force(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev,
                   int kick);
