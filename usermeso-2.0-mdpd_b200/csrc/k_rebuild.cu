@@ -278,12 +278,13 @@ __device__ __forceinline__ void bucket_warp(const BoxDesc &B, int *arr, int s, i
     __syncwarp();
 }
 
-// Buckets are taken four at a time per warp, one per group of 8 lanes: a bucket of up to 8
-// members (the usual case: a bin's locals split into two reorder classes, or a border bin) is
-// ordered with shuffles inside its group, so the warp waits once for the loads of four buckets;
-// a larger one is ordered by the whole warp afterwards.
+// Buckets are taken four at a time per warp, one per group of 8 lanes holding up to 4 members
+// each: a bucket of up to 32 members (the usual case: a reorder class is one bin's interior or
+// border locals, ~14 at rho 6.05) is ordered with shuffles inside its group, so the warp waits
+// once for the loads of four buckets; a larger one is ordered by the whole warp afterwards.
+constexpr int kGroupSlots = 4;  // members per lane of an 8-lane group
 template <int MODE>  // 0: reorder classes -> perm, 1: bins -> bin_order + bpos
-__global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict__ boxes,
+__global__ void __launch_bounds__(256, 4) k_rb_bucket(const BoxDesc *__restrict__ boxes,
                                                    const Unit *__restrict__ units, int nunits)
 {
     __shared__ unsigned long long s_key[8][kClassMax];
@@ -309,39 +310,56 @@ __global__ void __launch_bounds__(256, 5) k_rb_bucket(const BoxDesc *__restrict_
                 if (l8 == 0) cnt[b] = 0;  // check build: a bucket outside its array
                 n = 0;
             }
-            // a bin whose last member is a local holds locals only (they come first in a bin):
-            // it is already in index order; its test is loaded for the four bins at once
-            bool locals_only = false;
-            if (MODE == 1 && n > 8 && l8 == 0) locals_only = arr[s + n - 1] < B.nlocal;
-            const bool small = n > 0 && n <= 8;
-            const bool member = small && l8 < n;
-            int idx = 0;
-            unsigned long long k = ~0ull;
-            if (member) {
-                idx = MDPD_IDX(arr[s + l8], lim);
-                k = MODE == 0 ? (((unsigned long long)(uint32_t)B.sub_of[idx] << 32) | (uint32_t)idx)
-                              : (unsigned long long)(uint32_t)idx;
-            }
-            // bins of locals only are already in index order, bpos written by the scatter
-            bool keep_order = false;
             if (MODE == 1) {
-                const unsigned ghosts = __ballot_sync(0xffffffffu, member && idx >= B.nlocal);
-                keep_order = ((ghosts >> (grp * 8)) & 0xFFu) == 0;
+                // a bin whose last member is a local holds no ghost image (locals come first): it
+                // is already in index order, its bpos written by the scatter
+                int last = 0;
+                if (n > 0 && l8 == 0) last = arr[s + n - 1];
+                last = __shfl_sync(0xffffffffu, last, grp << 3);
+                if (n > 0 && last < B.nlocal) {
+                    if (l8 == 0) cnt[b] = 0;
+                    n = 0;
+                }
             }
-            int rank = 0;
+            const bool group = n > 0 && n <= 8 * kGroupSlots;
+            const int slots = __reduce_max_sync(0xffffffffu, group ? (n + 7) >> 3 : 0);  // warp-uniform
+            int idx[kGroupSlots];
+            unsigned long long k[kGroupSlots];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const unsigned long long kq = __shfl_sync(0xffffffffu, k, (grp << 3) | q);
-                rank += (q < n && kq < k) ? 1 : 0;
+            for (int m = 0; m < kGroupSlots; ++m) {
+                idx[m] = 0;
+                if (group && l8 + 8 * m < n) idx[m] = MDPD_IDX(arr[s + l8 + 8 * m], lim);
             }
-            if (member && !keep_order) {
-                arr[s + rank] = idx;
-                if (MODE == 1) B.bpos[s + rank] = list_pos(B.pos[idx], idx, B.nlocal);
+#pragma unroll
+            for (int m = 0; m < kGroupSlots; ++m) {
+                k[m] = ~0ull;  // no member: above every key, counted by no rank
+                if (group && l8 + 8 * m < n)
+                    k[m] = MODE == 0 ? (((unsigned long long)(uint32_t)B.sub_of[idx[m]] << 32) | (uint32_t)idx[m])
+                                     : (unsigned long long)(uint32_t)idx[m];
             }
-            if (small && l8 == 0) cnt[b] = 0;
-            // buckets of more than 8 members: the whole warp, one after another
-            if (locals_only) cnt[b] = 0;
-            unsigned big = __ballot_sync(0xffffffffu, l8 == 0 && n > 8 && !locals_only);
+            // rank of each member: the group's keys below it (every member's key is loaded before
+            // any lane gets past these shuffles, so the stores below cannot overwrite an unread one)
+            int rank[kGroupSlots] = {};
+#pragma unroll
+            for (int mm = 0; mm < kGroupSlots; ++mm) {
+                if (mm >= slots) break;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const unsigned long long kq = __shfl_sync(0xffffffffu, k[mm], (grp << 3) | q);
+#pragma unroll
+                    for (int m = 0; m < kGroupSlots; ++m) rank[m] += kq < k[m] ? 1 : 0;
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < kGroupSlots; ++m) {
+                if (group && l8 + 8 * m < n) {
+                    arr[s + rank[m]] = idx[m];
+                    if (MODE == 1) B.bpos[s + rank[m]] = list_pos(B.pos[idx[m]], idx[m], B.nlocal);
+                }
+            }
+            if (group && l8 == 0) cnt[b] = 0;
+            // buckets of more than 32 members: the whole warp, one after another
+            unsigned big = __ballot_sync(0xffffffffu, l8 == 0 && n > 8 * kGroupSlots);
             while (big) {
                 const int leader = __ffs(big) - 1;
                 big &= big - 1;
@@ -821,7 +839,7 @@ void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const S
     k_rb_key<<<g(u.local.n, r.key), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
     scan<kSelCls>(s, boxes, u.scan_cls, u.nbox, sms);
     k_rb_scatter_cls<<<g(u.local.n, r.cls), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
-    k_rb_bucket<0><<<g(u.cls.n, 5), 256, 0, s>>>(boxes, u.cls.d, u.cls.n);
+    k_rb_bucket<0><<<g(u.cls.n, 4), 256, 0, s>>>(boxes, u.cls.d, u.cls.n);
     if (c.style == 0)
         k_rb_permute<0><<<g(u.local.n, r.permute0), kUnit, 0, s>>>(boxes, u.local.d, u.local.n, u.nbox, done);
     else
@@ -830,7 +848,7 @@ void launch_rebuild(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const S
     k_rb_ghosts<<<g(u.local.n, r.ghosts), kUnit, 0, s>>>(boxes, u.local.d, u.local.n);
     scan<kSelBin>(s, boxes, u.scan_bin, u.nbox, sms);
     k_rb_scatter_bins<<<g(u.all.n, r.bins), kUnit, 0, s>>>(boxes, u.all.d, u.all.n);
-    k_rb_bucket<1><<<g(u.bins.n, 5), 256, 0, s>>>(boxes, u.bins.d, u.bins.n);
+    k_rb_bucket<1><<<g(u.bins.n, 4), 256, 0, s>>>(boxes, u.bins.d, u.bins.n);
     k_rb_list<<<g(u.bins.n * 32, 4), 256, 0, s>>>(boxes, u.bins.d, u.bins.n, u.nbox, done + 1);
 }
 
