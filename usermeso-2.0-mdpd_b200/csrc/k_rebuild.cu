@@ -214,13 +214,16 @@ __global__ void __launch_bounds__(256) k_scan_down(const BoxDesc *__restrict__ b
     }
 }
 
+// resident blocks per SM of the scan passes, from the occupancy API (init_rebuild_shapes)
+static int g_scan_reduce[3] = {4, 4, 4}, g_scan_down[3] = {4, 4, 4};
+
 template <int SEL>
 static void scan(cudaStream_t s, BoxDesc *boxes, const UnitList &ul, int nbox, int sms)
 {
-    const int grid = ul.n < sms * 4 ? (ul.n > 0 ? ul.n : 1) : sms * 4;
-    k_scan_reduce<SEL><<<grid, 256, 0, s>>>(boxes, ul.d, ul.n);
+    auto g = [&](int per_sm) { return ul.n < sms * per_sm ? (ul.n > 0 ? ul.n : 1) : sms * per_sm; };
+    k_scan_reduce<SEL><<<g(g_scan_reduce[SEL]), 256, 0, s>>>(boxes, ul.d, ul.n);
     k_scan_top<SEL><<<nbox, 256, 0, s>>>(boxes, nbox);
-    k_scan_down<SEL><<<grid, 256, 0, s>>>(boxes, ul.d, ul.n);
+    k_scan_down<SEL><<<g(g_scan_down[SEL]), 256, 0, s>>>(boxes, ul.d, ul.n);
 }
 
 // ---------------------------------------------------------------------------
@@ -808,12 +811,12 @@ struct RebuildShapes {
 static RebuildShapes g_shapes;
 static std::once_flag g_shapes_once;
 
-template <typename K> static int resident_blocks(K kernel)
+template <typename K> static int resident_blocks(K kernel, int threads = kUnit, int fallback = 8)
 {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kUnit, 0) != cudaSuccess || b < 1) {
-        (void)cudaGetLastError();  // a failed query leaves the fixed 8
-        return 8;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, 0) != cudaSuccess || b < 1) {
+        (void)cudaGetLastError();  // a failed query leaves the fixed grid
+        return fallback;
     }
     return b;
 }
@@ -827,6 +830,12 @@ void init_rebuild_shapes()
         g_shapes.permute1 = resident_blocks(k_rb_permute<1>);
         g_shapes.ghosts = resident_blocks(k_rb_ghosts);
         g_shapes.bins = resident_blocks(k_rb_scatter_bins);
+        g_scan_reduce[0] = resident_blocks(k_scan_reduce<0>, 256, 4);
+        g_scan_reduce[1] = resident_blocks(k_scan_reduce<1>, 256, 4);
+        g_scan_reduce[2] = resident_blocks(k_scan_reduce<2>, 256, 4);
+        g_scan_down[0] = resident_blocks(k_scan_down<0>, 256, 4);
+        g_scan_down[1] = resident_blocks(k_scan_down<1>, 256, 4);
+        g_scan_down[2] = resident_blocks(k_scan_down<2>, 256, 4);
     });
 }
 

@@ -572,29 +572,38 @@ void launch_force(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const Ste
 // slots: 0 sum m v^2 (all), 1..6 virial xx yy zz xy xz yz (force pass), 7 pair energy,
 // 8..10 momentum, 11 sum m v^2 over the nve group, 12..17 kinetic tensor xx yy zz xy xz yz.
 // ---------------------------------------------------------------------------
+// A block takes a group of kThermoGroup consecutive units of a box (the group's first unit; the
+// others of the group are skipped): each thread sums its particles i, i + kUnit, ... in that
+// order, then the warp and block trees; the sums go to the group's first partial row and zeros
+// to the others, so the per-box tree of k_thermo_sum is unchanged.  The structure depends only
+// on particle indices: the sums are the same bits for any grid.
+constexpr int kThermoGroup = 8;
 __global__ void __launch_bounds__(kUnit) k_thermo_units(const BoxDesc *__restrict__ boxes,
                                                         const Unit *__restrict__ units, int nunits)
 {
     constexpr int NQ = 11;
     __shared__ double s_red[kUnit / 32][NQ];
-    const int slot[NQ] = {0, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17};
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const Unit U = units[u];
+        const int row = U.begin / kUnit;
+        if (row % kThermoGroup != 0) continue;  // taken by its group's first unit
         const BoxDesc &B = boxes[U.box];
         const int c = B.st->cur;
-        const int i = U.begin + threadIdx.x;
+        const int end = min(U.begin + kThermoGroup * kUnit, B.nlocal);
         double vals[NQ];
 #pragma unroll
         for (int q = 0; q < NQ; ++q) vals[q] = 0.0;
-        if (i < U.end) {
+#pragma unroll 4
+        for (int i = U.begin + threadIdx.x; i < end; i += kUnit) {
             const int t = B.type[c][i];
             const double m = B.mass[t - 1];
             const double vx = B.v[c][0][i], vy = B.v[c][1][i], vz = B.v[c][2][i];
-            vals[0] = m * (vx * vx + vy * vy + vz * vz);
-            vals[1] = m * vx, vals[2] = m * vy, vals[3] = m * vz;
-            if (B.mask[c][i] & B.nve_bit) vals[4] = vals[0];
-            vals[5] = m * vx * vx, vals[6] = m * vy * vy, vals[7] = m * vz * vz;
-            vals[8] = m * vx * vy, vals[9] = m * vx * vz, vals[10] = m * vy * vz;
+            const double ke = m * (vx * vx + vy * vy + vz * vz);
+            vals[0] += ke;
+            vals[1] += m * vx, vals[2] += m * vy, vals[3] += m * vz;
+            if (B.mask[c][i] & B.nve_bit) vals[4] += ke;
+            vals[5] += m * vx * vx, vals[6] += m * vy * vy, vals[7] += m * vz * vz;
+            vals[8] += m * vx * vy, vals[9] += m * vx * vz, vals[10] += m * vy * vz;
         }
 #pragma unroll
         for (int q = 0; q < NQ; ++q)
@@ -602,10 +611,14 @@ __global__ void __launch_bounds__(kUnit) k_thermo_units(const BoxDesc *__restric
         if ((threadIdx.x & 31) == 0)
             for (int q = 0; q < NQ; ++q) s_red[threadIdx.x / 32][q] = vals[q];
         __syncthreads();
-        if (threadIdx.x < NQ) {
+        const int rows = (B.nlocal + kUnit - 1) / kUnit;
+        for (int k = threadIdx.x; k < NQ * kThermoGroup; k += blockDim.x) {
+            const int q = k % NQ, r = row + k / NQ;
+            if (r >= rows) continue;
             double a = 0.0;
-            for (int w = 0; w < kUnit / 32; ++w) a += s_red[w][threadIdx.x];
-            B.partial[(size_t)(U.begin / kUnit) * kPartialStride + slot[threadIdx.x]] = a;
+            if (r == row)
+                for (int w = 0; w < kUnit / 32; ++w) a += s_red[w][q];
+            B.partial[(size_t)r * kPartialStride + (q == 0 ? 0 : q + 7)] = a;  // slots 0, 8..17
         }
         __syncthreads();
     }
