@@ -204,12 +204,9 @@ __device__ __forceinline__ void ev_to_partial(const BoxDesc &B, const Unit &U, c
 {
     // every pair once, full weight (the reference halves each side's share)
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    double vals[7] = {ev.vxx, ev.vyy, ev.vzz, ev.vxy, ev.vxz, ev.vyz, ev.pe};
-#pragma unroll
-    for (int q = 0; q < 7; ++q)
-        for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_down_sync(0xffffffffu, vals[q], o);
-    if (lane == 0)
-        for (int q = 0; q < 7; ++q) red[w][q] = vals[q];
+    double vals[8] = {ev.vxx, ev.vyy, ev.vzz, ev.vxy, ev.vxz, ev.vyz, ev.pe, 0.0};
+    const double tot = warp_sum_spread(vals);  // the warp's total of value lane / 4
+    if ((lane & 3) == 0 && (lane >> 2) < 7) red[w][lane >> 2] = tot;
     __syncthreads();
     if (t < 7) {
         double a = 0.0;

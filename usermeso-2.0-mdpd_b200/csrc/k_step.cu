@@ -497,18 +497,15 @@ __global__ void __launch_bounds__(kUnit *TPP, 8 / TPP) k_force(const BoxDesc *__
         }
         if (EV) {
             // per-unit FP64 partials in a fixed order (deterministic)
-            double vals[7] = {0, 0, 0, 0, 0, 0, 0};
+            double vals[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             if (live && t == 0) {
                 vals[0] = 0.5 * ev.vxx, vals[1] = 0.5 * ev.vyy, vals[2] = 0.5 * ev.vzz;
                 vals[3] = 0.5 * ev.vxy, vals[4] = 0.5 * ev.vxz, vals[5] = 0.5 * ev.vyz;
                 vals[6] = 0.5 * ev.pe;
             }
-#pragma unroll
-            for (int q = 0; q < 7; ++q)
-                for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_down_sync(0xffffffffu, vals[q], o);
-            const int w = threadIdx.x / 32;
-            if ((threadIdx.x & 31) == 0)
-                for (int q = 0; q < 7; ++q) s_red[w][q] = vals[q];
+            const double tot = warp_sum_spread(vals);  // the warp's total of value lane / 4
+            const int w = threadIdx.x / 32, lane = threadIdx.x & 31;
+            if ((lane & 3) == 0 && (lane >> 2) < 7) s_red[w][lane >> 2] = tot;
             __syncthreads();
             if (threadIdx.x < 7) {
                 double a = 0.0;
@@ -581,7 +578,7 @@ constexpr int kThermoGroup = 8;
 __global__ void __launch_bounds__(kUnit) k_thermo_units(const BoxDesc *__restrict__ boxes,
                                                         const Unit *__restrict__ units, int nunits)
 {
-    constexpr int NQ = 11;
+    constexpr int NQ = 11;  // sums, padded to 16 for the warp reduction
     __shared__ double s_red[kUnit / 32][NQ];
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const Unit U = units[u];
@@ -590,9 +587,9 @@ __global__ void __launch_bounds__(kUnit) k_thermo_units(const BoxDesc *__restric
         const BoxDesc &B = boxes[U.box];
         const int c = B.st->cur;
         const int end = min(U.begin + kThermoGroup * kUnit, B.nlocal);
-        double vals[NQ];
+        double vals[16];
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) vals[q] = 0.0;
+        for (int q = 0; q < 16; ++q) vals[q] = 0.0;
 #pragma unroll 4
         for (int i = U.begin + threadIdx.x; i < end; i += kUnit) {
             const int t = B.type[c][i];
@@ -605,11 +602,9 @@ __global__ void __launch_bounds__(kUnit) k_thermo_units(const BoxDesc *__restric
             vals[5] += m * vx * vx, vals[6] += m * vy * vy, vals[7] += m * vz * vz;
             vals[8] += m * vx * vy, vals[9] += m * vx * vz, vals[10] += m * vy * vz;
         }
-#pragma unroll
-        for (int q = 0; q < NQ; ++q)
-            for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_down_sync(0xffffffffu, vals[q], o);
-        if ((threadIdx.x & 31) == 0)
-            for (int q = 0; q < NQ; ++q) s_red[threadIdx.x / 32][q] = vals[q];
+        const double tot = warp_sum_spread(vals);  // the warp's total of value lane / 2
+        const int lane = threadIdx.x & 31;
+        if ((lane & 1) == 0 && (lane >> 1) < NQ) s_red[threadIdx.x / 32][lane >> 1] = tot;
         __syncthreads();
         const int rows = (B.nlocal + kUnit - 1) / kUnit;
         for (int k = threadIdx.x; k < NQ * kThermoGroup; k += blockDim.x) {

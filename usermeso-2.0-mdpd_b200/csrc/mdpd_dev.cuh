@@ -424,6 +424,33 @@ __device__ __forceinline__ unsigned long long dist2x2(unsigned long long dx, uns
     return fma2(dz, dz, fma2(dx, dx, mul2(dy, dy)));
 }
 
+// Warp sums of N values (N a power of two, 2..32) by recursive halving: at each of log2(N)
+// steps lanes pair across bit o (16, 8, ...), each keeps half of its values and adds the
+// partner's copy of that half, so a step moves half as many values as the last; a plain
+// butterfly over the remaining lane bits ends it.  N - 1 + (5 - log2 N) shuffles instead of
+// 5 N.  Returns, in every lane, the warp's total of value (lane >> (5 - log2 N)) & (N - 1).
+// The order of the additions is fixed: the same bits on every run.
+template <int N> __device__ __forceinline__ double warp_sum_spread(double (&v)[N])
+{
+    static_assert(N >= 2 && N <= 32 && (N & (N - 1)) == 0, "N: a power of two up to 32");
+    const int lane = threadIdx.x & 31;
+    int o = 16;
+#pragma unroll
+    for (int len = N; len > 1; len >>= 1, o >>= 1) {
+        const bool upper = lane & o;  // keeps values [len/2, len), renumbered from 0
+#pragma unroll
+        for (int k = 0; k < len / 2; ++k) {
+            const double give = upper ? v[k] : v[k + len / 2];
+            const double keep = upper ? v[k + len / 2] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xffffffffu, give, o);
+        }
+    }
+    double r = v[0];
+#pragma unroll
+    for (; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    return r;
+}
+
 // ---------------------------------------------------------------------------
 // Index checks of the check build (compiled with -DMDPD_CHECK; `build.py --check` writes
 // libmdpd_check.so).  MDPD_IDX(i, n) is i when 0 <= i < n; otherwise it sets kErrIndex in the
