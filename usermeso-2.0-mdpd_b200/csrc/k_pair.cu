@@ -13,9 +13,11 @@
 //   the particle and its ghost images for the force pass's gathers.
 // k_force_pairs: the 32 compact rows of a warp are concatenated and split into 32 equal
 //   contiguous shares, one per lane (a prefix scan of the row lengths and one binary search), so
-//   every lane evaluates the same number of pairs whatever the row lengths.  Each entry carries
-//   j's type; j's (x, y, z, rho) and velocity/signature are two float4 gathers, loaded for the
-//   next pair while the current one is evaluated.  The mDPD pair force (pair_mdpd_meso.cu:139-225)
+//   every lane evaluates the same number of pairs whatever the row lengths.  The concatenated
+//   rows are first staged in shared memory by coalesced loads (consecutive lanes, consecutive
+//   entries), so the pair loop's entry reads (each lane in a different row) do not touch 32
+//   table lines each.  Each entry carries j's type; j's (x, y, z, rho) and velocity/signature are
+//   two float4 gathers, loaded for the next pair while the current one is evaluated.  The mDPD pair force (pair_mdpd_meso.cu:139-225)
 //   is summed for the row in 64-bit fixed point (2^-32 units) in registers and flushed when the
 //   lane's share moves to the next row; -F goes to j's source particle in the same fixed point,
 //   through shared memory when the source is one of the block's 128 rows and global 64-bit
@@ -166,6 +168,10 @@ __device__ __forceinline__ unsigned long long join64(unsigned lo, unsigned hi)
     return ((unsigned long long)hi << 32) | lo;
 }
 
+// compact entries a warp stages in shared memory: its 32 rows hold ~400 at rho 6.05 (12.6 owned
+// force-range pairs each); a warp with more reads them from the table
+constexpr int kWarpEntries = 640;
+
 // shared memory of the global-index force pass
 struct RowsSmem {
     PairCoeff coeff[kMaxTypes * kMaxTypes];
@@ -174,6 +180,7 @@ struct RowsSmem {
     int pre[4][33];
     unsigned lo[3][128], hi[3][128];
     double red[4][7];
+    int ent[4][kWarpEntries];  // each warp's concatenated compact rows (when they fit)
 };
 
 // the warp's rows [wb, wb + 32) as one list of T entries split into 32 equal shares; P: prefix
@@ -241,6 +248,18 @@ __device__ __forceinline__ void force_pairs(const BoxDesc &B, const Unit &U, Row
     unsigned long long *fax = B.facc, *fay = B.facc + nlocal, *faz = B.facc + 2 * nlocal;
     EvAcc ev = {0, 0, 0, 0, 0, 0, 0};
     bool bad = false;
+    // the warp's rows, concatenated, into shared memory: consecutive lanes load consecutive
+    // entries (a row's entries are contiguous in the table), so the pair loop's entry reads,
+    // one per lane in 32 different rows, come from shared memory instead of 32 table lines
+    const bool staged = T <= kWarpEntries;  // warp-uniform
+    int *const ent = S.ent[w];
+    if (staged) {
+        for (int m = lane; m < T; m += 32) {
+            const int r = row_of(P, m);
+            ent[m] = __ldcs(B.table2 + (size_t)(i0 + r) * ncol2 + (m - P[r]));
+        }
+        __syncwarp();
+    }
     if (m0 < m1) {
         int r = row_of(P, m0);
         int rbeg = P[r], rend = P[r + 1];
@@ -248,7 +267,7 @@ __device__ __forceinline__ void force_pairs(const BoxDesc &B, const Unit &U, Row
         float rho_i = S.rho[wb + r];
         long long ax = 0, ay = 0, az = 0;
         // j's state for the next entry is loaded while the current pair is evaluated
-        const int en = __ldcs(B.table2 + (size_t)(i0 + r) * ncol2 + (m0 - rbeg));
+        const int en = staged ? ent[m0] : __ldcs(B.table2 + (size_t)(i0 + r) * ncol2 + (m0 - rbeg));
         int jn = MDPD_IDX(en & kEntryIndex, n_all(B)), tn = en >> kEntryTypeShift;
         float4 pjn = __ldg(&B.posrho[jn]), vjn = __ldg(&B.vel[jn]);
         int srcn = jn < nlocal ? jn : MDPD_IDX(__ldg(&B.gsrc[jn - nlocal]), nlocal);
@@ -269,13 +288,18 @@ __device__ __forceinline__ void force_pairs(const BoxDesc &B, const Unit &U, Row
             const int src = srcn, tj = tn;
             const float4 pj = pjn, vj = vjn;  // pj.w: rho of j
             if (m + 1 < m1) {
-                int rr = r, rb = rbeg, re = rend;  // entry m + 1: row r or a later non-empty row
-                while (m + 1 >= re) {
-                    ++rr;
-                    rb = re;
-                    re = P[rr + 1];
+                int e;
+                if (staged) {
+                    e = ent[m + 1];
+                } else {
+                    int rr = r, rb = rbeg, re = rend;  // entry m + 1: row r or a later non-empty row
+                    while (m + 1 >= re) {
+                        ++rr;
+                        rb = re;
+                        re = P[rr + 1];
+                    }
+                    e = __ldcs(B.table2 + (size_t)(i0 + rr) * ncol2 + (m + 1 - rb));
                 }
-                const int e = __ldcs(B.table2 + (size_t)(i0 + rr) * ncol2 + (m + 1 - rb));
                 const int jj = MDPD_IDX(e & kEntryIndex, n_all(B));
                 tn = e >> kEntryTypeShift;
                 pjn = __ldg(&B.posrho[jj]);
