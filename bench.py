@@ -298,7 +298,7 @@ def main():
                        "parallelism": f"{world} GPU(s), {256 * world} boxes placed by mdpd_place "
                                       "(no data-path collective)",
                        "tuned": {"density_gathers_in_flight": shape_density,
-                                 "force_lanes_per_warp_share": shape_force}},
+                                 "force_rows_staged": shape_force == 32}},
             "clocks": clk.summary(), "gpu_launches": gpu_launches}
 
     if not args.no_extras:
@@ -392,7 +392,7 @@ def main():
                             "density_frac": B_RHO * n4 / (prof["density_ms"] / 1e3) / 1e9 / peak,
                             "force_frac": B_F * n4 / (prof["force_ms"] / 1e3) / 1e9 / peak,
                             "integrate_ms": prof["integrate_ms"], "rebuild_ms_avg": prof["rebuild_ms"],
-                            "tuned": {"density_gathers_in_flight": tuned4[0], "force_lanes_per_warp_share": tuned4[1]}}
+                            "tuned": {"density_gathers_in_flight": tuned4[0], "force_rows_staged": tuned4[1] == 32}}
         line["single_box_4M"] = {"value": n4 / (ms4 / 1e3), "unit": "particle-steps/s", "ms_per_step": ms4,
                                  "step_frac": B_STEP * n4 / (ms4 / 1e3) / 1e9 / peak,
                                  "note": "whole graph step (rebuilds amortised) against the step's algorithmic "

@@ -162,9 +162,11 @@ int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int
 int mdpd_batch_run_thermo(mdpd_batch_t *b, int64_t nsteps, mdpd_thermo_t *out, int64_t *d2h_bytes_per_step);
 /* project autotuner: times the candidate shapes of the pair passes on this batch (13 real steps
  * each, so the boxes advance) and keeps the fastest. Pair-once mDPD batches: *shape_density =
- * neighbour gathers in flight per lane in the density pass (4, 6 or 8), *shape_force = 32 (a
- * warp shares its 32 particles' pairs out to its 32 lanes; fixed). Full-list batches (classic
- * DPD, wall-coupled mDPD): threads per particle of the density and force passes (1, 2 or 4 each). */
+ * neighbour gathers in flight per lane in the density pass (4, 6 or 8); *shape_force = 32 (a
+ * warp shares its 32 particles' pairs out to its 32 lanes, its compact rows staged in shared
+ * memory first) or 0 (the same shares, each entry read from the table in the pair loop).
+ * Full-list batches (classic DPD, wall-coupled mDPD): threads per particle of the density and
+ * force passes (1, 2 or 4 each). */
 int mdpd_batch_tune(mdpd_batch_t *b, int32_t *shape_density, int32_t *shape_force);
 /* mdpd_batch_tune with its picks persisted in a JSON file (path; created when absent):
  * {"version": 1, "entries": {"<key>": {"density": D, "force": F, "ms_per_step": T}}}.  The key

@@ -163,7 +163,7 @@ def test_autotuner_picks_a_shape_and_keeps_the_physics():
     b.setup()
     b.step(20)
     g, f = b.tune()
-    assert g in (4, 6, 8) and f == 32
+    assert g in (4, 6, 8) and f in (0, 32)
     b.step(20)
     for k in range(4):
         t = b.thermo(k)
@@ -242,8 +242,8 @@ def test_tune_cache_persists_the_pick(tmp_path):
     b = mdpd.Batch(sp)
     b.setup()
     d, f, hit = b.tune(cache=cache)
-    assert not hit and d in (4, 6, 8) and f == 32
-    assert b.thermo(0).step == 39  # three candidates, 13 timed steps each
+    assert not hit and d in (4, 6, 8) and f in (0, 32)
+    assert b.thermo(0).step == 78  # six candidates, 13 timed steps each
     doc = json.loads(cache.read_text())
     (key, entry), = doc["entries"].items()
     assert "pair-once" in key and entry["density"] == d and entry["ms_per_step"] > 0

@@ -304,6 +304,28 @@ def test_density_shapes_give_the_same_bits():
     lam.close()
 
 
+def test_staged_and_table_force_entries_give_the_same_bits():
+    # the pair-once force pass stages each warp's compact rows in shared memory (pair_modify stage
+    # yes, the default) or reads each entry from the table in the pair loop (stage no, also the
+    # path of a warp whose rows exceed the staging capacity): the same pairs in the same per-lane
+    # order, so forces and 50 steps of trajectory are bitwise the same
+    out = []
+    for st in ("yes", "no"):
+        lam = mdpd_box(n=4000, extra=f"pair_modify stage {st}")
+        lam.setup()
+        f = lam.field("force")
+        lam.step(50)
+        x, v, _, _ = lam.state()
+        out.append((f, x, v))
+        lam.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+    lam = mdpd.Lammps()
+    with pytest.raises(mdpd.MdpdError):
+        lam.command("pair_modify stage maybe")
+    lam.close()
+
+
 def test_two_type_pair_once_force_and_density_match_oracle():
     # the pair-once passes with two atom types (coefficients looked up per type pair, masses per
     # type in the density): sigma = 0 forces and the density against the FP64 oracle

@@ -563,12 +563,15 @@ int mdpd_batch_time(mdpd_batch_t *b, int64_t nsteps, double *ms)
 static std::vector<StepConfig> tune_candidates(const StepConfig &base)
 {
     std::vector<StepConfig> cands;
-    if (base.half) {  // pair-once passes: the density pass's gathers in flight
-        for (int g : {4, 6, 8}) {
-            StepConfig c = base;
-            c.gather = g;
-            cands.push_back(c);
-        }
+    if (base.half) {  // pair-once passes: the density pass's gathers in flight, the force
+                      // pass's entries staged in shared memory or read from the table
+        for (int g : {4, 6, 8})
+            for (int st : {1, 0}) {
+                StepConfig c = base;
+                c.gather = g;
+                c.stage_rows = st;
+                cands.push_back(c);
+            }
     } else {  // full-list passes: threads per particle of each pass
         for (int td : {1, 2, 4})
             for (int tf : {1, 2, 4}) {
@@ -585,7 +588,7 @@ static TunePick pick_of(const StepConfig &c, double ms)
 {
     TunePick p;
     p.density = c.half ? c.gather : c.tpp_density;
-    p.force = c.half ? 32 : c.tpp_force;
+    p.force = c.half ? (c.stage_rows ? 32 : 0) : c.tpp_force;
     p.ms_per_step = ms;
     return p;
 }

@@ -223,7 +223,7 @@ __device__ __forceinline__ void ev_to_partial(const BoxDesc &B, const Unit &U, c
 }
 
 template <bool EXACT, bool EV, bool UNI>
-__device__ __forceinline__ void force_pairs(const BoxDesc &B, const Unit &U, RowsSmem &S)
+__device__ __forceinline__ void force_pairs(const BoxDesc &B, const Unit &U, RowsSmem &S, int stage_cap)
 {
     const int t = threadIdx.x, lane = t & 31, w = t >> 5, wb = t & ~31;
     for (int q = t; q < (UNI ? 1 : B.ntype * B.ntype); q += blockDim.x) S.coeff[q] = B.coeff[q];
@@ -251,7 +251,7 @@ __device__ __forceinline__ void force_pairs(const BoxDesc &B, const Unit &U, Row
     // the warp's rows, concatenated, into shared memory: consecutive lanes load consecutive
     // entries (a row's entries are contiguous in the table), so the pair loop's entry reads,
     // one per lane in 32 different rows, come from shared memory instead of 32 table lines
-    const bool staged = T <= kWarpEntries;  // warp-uniform
+    const bool staged = T <= stage_cap;  // warp-uniform; stage_cap is kWarpEntries, or 0 to read the table
     int *const ent = S.ent[w];
     if (staged) {
         for (int m = lane; m < T; m += 32) {
@@ -344,13 +344,14 @@ __device__ __forceinline__ void force_pairs(const BoxDesc &B, const Unit &U, Row
 // 7 blocks per SM (up to 72 registers, no spill) measured fastest against 6 and 8
 template <bool EXACT, bool EV, bool UNI>
 __global__ void __launch_bounds__(128, 7) k_force_pairs(const BoxDesc *__restrict__ boxes,
-                                                        const Unit *__restrict__ units, int nunits)
+                                                        const Unit *__restrict__ units, int nunits,
+                                                        int stage_cap)
 {
     __shared__ RowsSmem S;
     const int u = blockIdx.x;
     if (u >= nunits) return;
     const Unit U = units[u];
-    force_pairs<EXACT, EV, UNI>(boxes[U.box], U, S);
+    force_pairs<EXACT, EV, UNI>(boxes[U.box], U, S, min(stage_cap, kWarpEntries));
 }
 
 __global__ void __launch_bounds__(kUnit) k_finalize(const BoxDesc *__restrict__ boxes,
@@ -406,23 +407,24 @@ void launch_density_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, co
 }
 
 template <bool EXACT, bool EV, bool UNI>
-static void force_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u)
+static void force_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, int stage_cap)
 {
-    k_force_pairs<EXACT, EV, UNI><<<u.local.n, 128, 0, s>>>(boxes, u.local.d, u.local.n);
+    k_force_pairs<EXACT, EV, UNI><<<u.local.n, 128, 0, s>>>(boxes, u.local.d, u.local.n, stage_cap);
 }
 
 void launch_force_half(cudaStream_t s, BoxDesc *boxes, const BatchUnits &u, const StepConfig &c, int ev, int kick)
 {
     const int g = u.local.n;
     if (g <= 0) return;
+    const int cap = c.stage_rows ? kWarpEntries : 0;
     if (c.exact_rng) {
-        if (ev) force_half<true, true, false>(s, boxes, u);
-        else if (c.uniform_types) force_half<true, false, true>(s, boxes, u);
-        else force_half<true, false, false>(s, boxes, u);
+        if (ev) force_half<true, true, false>(s, boxes, u, cap);
+        else if (c.uniform_types) force_half<true, false, true>(s, boxes, u, cap);
+        else force_half<true, false, false>(s, boxes, u, cap);
     } else {
-        if (ev) force_half<false, true, false>(s, boxes, u);
-        else if (c.uniform_types) force_half<false, false, true>(s, boxes, u);
-        else force_half<false, false, false>(s, boxes, u);
+        if (ev) force_half<false, true, false>(s, boxes, u, cap);
+        else if (c.uniform_types) force_half<false, false, true>(s, boxes, u, cap);
+        else force_half<false, false, false>(s, boxes, u, cap);
     }
     k_finalize<<<g, kUnit, 0, s>>>(boxes, u.local.d, g, kick);
 }

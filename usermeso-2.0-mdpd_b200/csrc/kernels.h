@@ -36,6 +36,8 @@ struct StepConfig {
     int half = 0;          // mdpd without wall coupling: each pair evaluated once (k_pair.cu)
     int half_enabled = 1;  // allow the half-list passes (set per batch from the boxes)
     int gather = 6;        // pair-once density pass: neighbour positions in flight per lane (4, 6, 8)
+    int stage_rows = 1;    // pair-once force pass: each warp's compact rows staged in shared memory
+                           // (0: the pair loop reads its entries from the table)
     int aboundary = 0;     // fix aboundary/meso at the end of each step
     int sms = 148;
 };

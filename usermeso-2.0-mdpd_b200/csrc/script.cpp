@@ -666,13 +666,18 @@ void Script::command(const std::string &raw)
         dirty_ = true;
     } else if (c == "pair_modify") {
         // extensions: pair_modify rng exact|fast (FP64 bit-exact gaussian or FP32 transform);
-        // gather 4|6|8 pins the pair-once density pass's neighbour gathers in flight per lane
+        // gather 4|6|8 pins the pair-once density pass's neighbour gathers in flight per lane;
+        // stage yes|no stages each warp's compact rows in shared memory for the pair-once force
+        // pass, or has its pair loop read them from the table
         for (int k = 1; k + 1 <= narg; k += 2) {
             if (a[k] == "rng") spec_.exact_rng = a[k + 1] == "exact";
             else if (a[k] == "gather") {
                 const int g = inum(a[k + 1]);
                 if (g != 4 && g != 6 && g != 8) parse_error("pair_modify gather must be 4, 6 or 8");
                 cfg.gather = g;
+            } else if (a[k] == "stage") {
+                if (a[k + 1] != "yes" && a[k + 1] != "no") parse_error("pair_modify stage must be yes or no");
+                cfg.stage_rows = a[k + 1] == "yes";
             }
         }
         dirty_ = true;
