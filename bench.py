@@ -268,7 +268,7 @@ def main():
     b = mdpd.Batch(specs, device=local)
     b.setup()
     b.step(args.equil)  # relax the random start (untimed)
-    shape_density, shape_force = b.tune()  # project autotuner (13 untimed steps per candidate shape)
+    shape_density, shape_force = b.tune()  # project autotuner (pair passes timed on the current state)
     b.step(args.warmup)
     r0 = b.rebuild_steps()
     barrier()
@@ -291,7 +291,7 @@ def main():
             "vs_baseline": None, "dtype": "f32 pair / f64 integrate", "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD, "boxes": len(cfg), "particles_per_gpu": ntot,
                        "start": f"uniform random positions, Maxwell velocities, {args.equil} untimed steps, "
-                                "then the autotuner's 13 untimed steps per candidate shape",
+                                "then the autotuner (pair passes timed per candidate shape, no steps)",
                        "rebuild_steps_timed": r1 - r0,
                        "l2": "inputs larger than L2: state + lists of ~%d particles (%.1f GB)" % (
                            ntot, ntot * 1.1e-6),
@@ -372,7 +372,7 @@ def main():
         b4 = mdpd.Batch([s4], device=local)
         b4.setup()
         b4.step(args.equil)
-        tuned4 = b4.tune()  # the project autotuner's shape for this box (13 untimed steps per candidate)
+        tuned4 = b4.tune()  # the project autotuner's shape for this box (pair passes timed per candidate)
         b4.step(args.warmup)
         torch.cuda.nvtx.range_push("pair_profile")  # ncu --nvtx-include pair_profile/: the launch list
         prof = b4.profile(max(10, args.steps // 2))

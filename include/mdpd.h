@@ -160,8 +160,10 @@ int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int
  * bits seen in any step's thermo make the call return MDPD_ERR_NAN / MDPD_ERR_OVERFLOW after all
  * nsteps (the records still hold every step). */
 int mdpd_batch_run_thermo(mdpd_batch_t *b, int64_t nsteps, mdpd_thermo_t *out, int64_t *d2h_bytes_per_step);
-/* project autotuner: times the candidate shapes of the pair passes on this batch (13 real steps
- * each, so the boxes advance) and keeps the fastest. Pair-once mDPD batches: *shape_density =
+/* project autotuner: times the candidate shapes of the pair passes on this batch's current state
+ * (each candidate's density and force passes evaluated once untimed and five times timed; they
+ * recompute the same forces, so the boxes do not advance) and keeps the fastest. Pair-once mDPD
+ * batches: *shape_density =
  * neighbour gathers in flight per lane in the density pass (4, 6 or 8); *shape_force = 32 (a
  * warp shares its 32 particles' pairs out to its 32 lanes, its compact rows staged in shared
  * memory first) or 0 (the same shares, each entry read from the table in the pair loop).
@@ -169,11 +171,12 @@ int mdpd_batch_run_thermo(mdpd_batch_t *b, int64_t nsteps, mdpd_thermo_t *out, i
  * force passes (1, 2 or 4 each). */
 int mdpd_batch_tune(mdpd_batch_t *b, int32_t *shape_density, int32_t *shape_force);
 /* mdpd_batch_tune with its picks persisted in a JSON file (path; created when absent):
- * {"version": 1, "entries": {"<key>": {"density": D, "force": F, "ms_per_step": T}}}.  The key
+ * {"version": 1, "entries": {"<key>": {"density": D, "force": F, "ms_per_step": T}}} (T: the pick's pair
+ * passes, ms per evaluation).  The key
  * names the workload class the pick applies to: GPU model and SM count, pass family and options,
  * mean density (0.25 steps), neighbour cutoff (0.05 steps), total particles and box count (powers
- * of two).  A stored key is applied without stepping the boxes (*cached = 1); otherwise the batch
- * is timed as by mdpd_batch_tune and its pick added to the file (*cached = 0), which is rewritten
+ * of two).  A stored key is applied without timing (*cached = 1); otherwise the batch is timed
+ * as by mdpd_batch_tune and its pick added to the file (*cached = 0), which is rewritten
  * whole through a temporary and a rename, keeping the other members.  A malformed file or entry
  * returns MDPD_ERR_PARSE and is left untouched.  The reference's ThreadTuner learns online and
  * keeps nothing across runs (autotuner_meso.h:11-96). */

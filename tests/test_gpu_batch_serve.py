@@ -164,7 +164,8 @@ def test_autotuner_picks_a_shape_and_keeps_the_physics():
     b.step(20)
     g, f = b.tune()
     assert g in (4, 6, 8) and f in (0, 32)
-    b.step(20)
+    assert b.thermo(0).step == 20  # tuning times the pair passes on the state: no steps
+    b.step(100)  # relaxation from the random start
     for k in range(4):
         t = b.thermo(k)
         assert t.status == 0 and 0.5 < t.temp < 2.0
@@ -178,6 +179,29 @@ def test_autotuner_picks_a_shape_and_keeps_the_physics():
     d.step(20)
     assert d.thermo(0).status == 0
     d.close()
+
+
+def test_tuning_leaves_the_state_as_it_was():
+    # the autotuner evaluates each candidate's pair passes on the current state (no kick): the
+    # forces it leaves are the ones the last step computed, so a tuned batch steps on bitwise as
+    # a batch pinned to the same shapes without tuning
+    sp = specs()
+    a = mdpd.Batch(sp)
+    a.setup()
+    a.step(20)
+    d, f = a.tune()
+    a.step(30)
+    b = mdpd.Batch(sp)
+    b.setup()
+    b.step(20)
+    b.set_shapes(d, f)
+    b.step(30)
+    for k in range(len(sp)):
+        xa, va = a.state(k)
+        xb, vb = b.state(k)
+        assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+    a.close()
+    b.close()
 
 
 def test_box_beyond_the_table_limit_is_refused():
@@ -243,7 +267,7 @@ def test_tune_cache_persists_the_pick(tmp_path):
     b.setup()
     d, f, hit = b.tune(cache=cache)
     assert not hit and d in (4, 6, 8) and f in (0, 32)
-    assert b.thermo(0).step == 78  # six candidates, 13 timed steps each
+    assert b.thermo(0).step == 0  # the candidates' pair passes are timed on the state: no steps
     doc = json.loads(cache.read_text())
     (key, entry), = doc["entries"].items()
     assert "pair-once" in key and entry["density"] == d and entry["ms_per_step"] > 0

@@ -593,7 +593,9 @@ static TunePick pick_of(const StepConfig &c, double ms)
     return p;
 }
 
-// time every candidate on the batch (3 + 10 real steps each) and keep the fastest
+// time every candidate's pair passes on the batch's current state (one untimed and five timed
+// evaluations; the same work for every candidate, and the boxes do not advance) and keep the
+// fastest; the pick's ms is its pair passes' time per evaluation
 static TunePick tune_by_timing(mdpd_batch_s *b)
 {
     const StepConfig base = b->batch->cfg;
@@ -601,22 +603,11 @@ static TunePick tune_by_timing(mdpd_batch_s *b)
     StepConfig pick = base;
     for (const StepConfig &c : tune_candidates(base)) {
         b->batch->reconfigure(c);
-        b->batch->run(3, true);
-        cudaEvent_t e0, e1;
-        check_cuda(cudaEventCreate(&e0), "event");
-        check_cuda(cudaEventCreate(&e1), "event");
-        cudaEventRecord(e0, b->batch->stream());
-        b->batch->run(10, false);
-        cudaEventRecord(e1, b->batch->stream());
-        cudaEventSynchronize(e1);
-        float t = 0;
-        cudaEventElapsedTime(&t, e0, e1);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
+        const double t = b->batch->time_pair_passes(5);
         if (t < best) best = t, pick = c;
     }
     b->batch->reconfigure(pick);
-    return pick_of(pick, best / 10.0);
+    return pick_of(pick, best);
 }
 
 // the workload class a stored pick applies to: GPU model and SM count, the pass family and

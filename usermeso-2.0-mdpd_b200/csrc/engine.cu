@@ -737,6 +737,29 @@ long long Batch::rebuild_steps()
     return h[3];
 }
 
+double Batch::time_pair_passes(int reps)
+{
+    Range r("mdpd::time_pair_passes");
+    cudaEvent_t e0, e1;
+    check_cuda(cudaEventCreate(&e0), "event");
+    check_cuda(cudaEventCreate(&e1), "event");
+    auto once = [&] {
+        if (cfg.style == 0) launch_density(stream_, d_boxes, units, cfg);
+        launch_force(stream_, d_boxes, units, cfg, 0, 0);
+    };
+    once();
+    check_cuda(cudaEventRecord(e0, stream_), "event");
+    for (int k = 0; k < reps; ++k) once();
+    check_cuda(cudaEventRecord(e1, stream_), "event");
+    check_cuda(cudaEventSynchronize(e1), "time pair passes");
+    float t = 0;
+    check_cuda(cudaEventElapsedTime(&t, e0, e1), "event");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_cuda(cudaGetLastError(), "time pair passes");
+    return t / reps;
+}
+
 void Batch::profile(long long nsteps, double out[5])
 {
     cudaEvent_t ev[5];

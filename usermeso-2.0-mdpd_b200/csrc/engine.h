@@ -139,6 +139,10 @@ public:
     // nsteps un-captured steps with CUDA events around each kernel group; per-step averages
     // in ms: [integrate, rebuild (all steps), density, force], plus steps that rebuilt
     void profile(long long nsteps, double out[5]);
+    // device ms of one evaluation of the pair passes (density, force without a kick) on the
+    // current state, averaged over reps after one untimed: the passes recompute the same forces,
+    // so the boxes do not advance (the autotuner's timing)
+    double time_pair_passes(int reps);
     long long rebuild_steps();             // steps whose rebuild body ran (device counter)
     void thermo(std::vector<Thermo> &out); // reduce + download (synchronous)
     // nsteps steps, each with energy and virial and followed by its thermo; sink(k, thermo) gets

@@ -362,9 +362,10 @@ class Batch:
         return n.value
 
     def tune(self, cache=None):
-        """pair-pass shapes (density, force) picked by timing the batch; with cache (a JSON file
-        path) a stored pick for this workload class is applied without stepping.  With cache the
-        result is (density, force, cached)."""
+        """pair-pass shapes (density, force) picked by timing the batch's pair passes on its
+        current state (the boxes do not advance); with cache (a JSON file path) a stored pick for
+        this workload class is applied without timing.  With cache the result is
+        (density, force, cached)."""
         a, b = C.c_int32(), C.c_int32()
         if cache is None:
             self._check(lib().mdpd_batch_tune(self.h, C.byref(a), C.byref(b)))
