@@ -329,8 +329,7 @@ def main():
         th, thermo_bytes = be.run_thermo(args.steps)
         temps = [[t.temp for t in row] for row in th]
         t2 = time.perf_counter()
-        for k in range(len(cfg)):
-            be.state(k, xout[k], vout[k])
+        be.states(xout, vout)  # every box's state with one call (mdpd_batch_get_states)
         e2e_s = time.perf_counter() - t0
         split = {"create_upload_setup_s": t1 - t0, "steps_s": t2 - t1, "download_s": e2e_s - (t2 - t0)}
         be.close()
@@ -344,7 +343,7 @@ def main():
                        "note": "wall clock of: create of all 256 boxes from pinned host x, v; setup; K steps, "
                                "each followed by a read of every box's thermo (mdpd_batch_run_thermo: step k's "
                                "thermo comes back while step k+1 runs); full state download into pinned host "
-                               "arrays",
+                               "arrays (mdpd_batch_get_states: every box with one call)",
                        "split": split}
         del temps, xin, vin, xout, vout
 

@@ -204,6 +204,21 @@ def test_tuning_leaves_the_state_as_it_was():
     b.close()
 
 
+def test_batch_states_equal_the_per_box_reads():
+    # mdpd_batch_get_states: every box's x, v with one call, the same arrays as one
+    # mdpd_batch_get_state per box; a null array is skipped
+    b = mdpd.Batch(specs())
+    b.setup()
+    b.step(25)
+    xs, vs = b.states()
+    for k in range(len(xs)):
+        x, v = b.state(k)
+        assert np.array_equal(xs[k], x) and np.array_equal(vs[k], v)
+    with pytest.raises(mdpd.MdpdError):
+        b._check(mdpd.lib().mdpd_batch_get_states(b.h, None, None, len(xs)))
+    b.close()
+
+
 def test_box_beyond_the_table_limit_is_refused():
     # the list kernels address a box's neighbour table with unsigned 32-bit offsets: a box whose
     # table would pass 2^32 entries (here through a density estimate that makes the rows long)

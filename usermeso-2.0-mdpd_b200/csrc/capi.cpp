@@ -537,6 +537,15 @@ int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int
     });
 }
 
+int mdpd_batch_get_states(mdpd_batch_t *b, double *const *x, double *const *v, int32_t nbox)
+{
+    if (!b || !x || !v || nbox != (int)b->boxes.size()) return MDPD_ERR_ARG;
+    return guard(b->err, [&] {
+        check_cuda(cudaSetDevice(b->device), "set device");
+        b->batch->download_all(x, v);
+    });
+}
+
 int mdpd_batch_time(mdpd_batch_t *b, int64_t nsteps, double *ms)
 {
     if (!b || !ms || nsteps <= 0) return MDPD_ERR_ARG;

@@ -453,18 +453,24 @@ void Box::release() noexcept
     arena_ = nullptr;
 }
 
+// both buffers of a box's x, v and tags: the tag gather picks the live one on the device
+static StateBuffers state_buffers(const BoxDesc &desc)
+{
+    StateBuffers sb;
+    for (int c = 0; c < 2; ++c) {
+        for (int k = 0; k < 3; ++k) sb.x[c][k] = desc.x[c][k], sb.v[c][k] = desc.v[c][k];
+        sb.tag[c] = desc.tag[c];
+    }
+    return sb;
+}
+
 void Box::download_by_tag(double *x, double *v, double *scratch) const
 {
     Range r("mdpd::download");
     double *d = scratch;
     if (!d) d = batch_alloc<double>(6 * (size_t)n, 0);  // the box pool, stream-ordered
     // the gather picks the live buffer on the device: one wait per call, at the end
-    StateBuffers sb;
-    for (int c = 0; c < 2; ++c) {
-        for (int k = 0; k < 3; ++k) sb.x[c][k] = desc.x[c][k], sb.v[c][k] = desc.v[c][k];
-        sb.tag[c] = desc.tag[c];
-    }
-    launch_gather_by_tag(0, sb, desc.st, n, d, d + 3 * (size_t)n);
+    launch_gather_by_tag(0, state_buffers(desc), desc.st, n, d, d + 3 * (size_t)n);
     check_cuda(cudaGetLastError(), "download");
     if (x) check_cuda(cudaMemcpyAsync(x, d, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, 0), "download");
     if (v) check_cuda(cudaMemcpyAsync(v, d + 3 * (size_t)n, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, 0),
@@ -885,6 +891,31 @@ void Batch::run_thermo(long long nsteps, const std::function<void(long long, con
 size_t Batch::thermo_bytes_per_step() const
 {
     return (sizeof(double) * kPartialStride + sizeof(BoxState)) * boxes_.size();
+}
+
+void Batch::download_all(double *const *x, double *const *v)
+{
+    Range r("mdpd::download_all");
+    size_t total = 0;
+    for (const Box *b : boxes_) total += 6 * (size_t)b->n;
+    if (total == 0) return;
+    double *d = batch_alloc<double>(total, stream_);
+    size_t off = 0;
+    for (const Box *b : boxes_) {
+        launch_gather_by_tag(stream_, state_buffers(b->desc), b->desc.st, b->n, d + off, d + off + 3 * (size_t)b->n);
+        off += 6 * (size_t)b->n;
+    }
+    check_cuda(cudaGetLastError(), "download gather");
+    off = 0;
+    for (size_t k = 0; k < boxes_.size(); ++k) {
+        const size_t n3 = 3 * (size_t)boxes_[k]->n;
+        if (x[k]) check_cuda(cudaMemcpyAsync(x[k], d + off, sizeof(double) * n3, cudaMemcpyDeviceToHost, stream_), "download");
+        if (v[k])
+            check_cuda(cudaMemcpyAsync(v[k], d + off + n3, sizeof(double) * n3, cudaMemcpyDeviceToHost, stream_), "download");
+        off += 2 * n3;
+    }
+    check_cuda(cudaFreeAsync(d, stream_), "download scratch");
+    check_cuda(cudaStreamSynchronize(stream_), "download");
 }
 
 void Batch::read_states(std::vector<BoxState> &out)

@@ -90,6 +90,7 @@ def lib():
             "mdpd_batch_setup": ([vp], C.c_int), "mdpd_batch_step": ([vp, i64], C.c_int),
             "mdpd_batch_thermo": ([vp, i32, C.POINTER(Thermo)], C.c_int),
             "mdpd_batch_get_state": ([vp, i32, dp, dp, i64], C.c_int),
+            "mdpd_batch_get_states": ([vp, C.POINTER(dp), C.POINTER(dp), i32], C.c_int),
             "mdpd_batch_tune": ([vp, i32p, i32p], C.c_int),
             "mdpd_batch_tune_cached": ([vp, cp, i32p, i32p, i32p], C.c_int),
             "mdpd_batch_set_shapes": ([vp, i32, i32], C.c_int),
@@ -409,6 +410,21 @@ class Batch:
         assert x.flags.c_contiguous and v.flags.c_contiguous
         self._check(lib().mdpd_batch_get_state(self.h, box, _ptr(x, C.c_double), _ptr(v, C.c_double), n))
         return x, v
+
+    def states(self, xs=None, vs=None):
+        """Every box's positions and velocities in tag order with one call (all copies back to back,
+        one wait); xs, vs: optional lists of preallocated C-contiguous float64 (n_k, 3) arrays."""
+        nb = len(self.n)
+        xs = [np.empty((n, 3)) for n in self.n] if xs is None else xs
+        vs = [np.empty((n, 3)) for n in self.n] if vs is None else vs
+        assert len(xs) == nb and len(vs) == nb
+        for a, n in zip(xs + vs, self.n + self.n):
+            assert a.shape == (n, 3) and a.dtype == np.float64 and a.flags.c_contiguous
+        dpt = C.POINTER(C.c_double)
+        px = (dpt * nb)(*[_ptr(a, C.c_double) for a in xs])
+        pv = (dpt * nb)(*[_ptr(a, C.c_double) for a in vs])
+        self._check(lib().mdpd_batch_get_states(self.h, px, pv, nb))
+        return xs, vs
 
     def close(self):
         if getattr(self, "h", None):
