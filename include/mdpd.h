@@ -154,9 +154,9 @@ int mdpd_batch_thermo_all(mdpd_batch_t *b, mdpd_thermo_t *out, int32_t nbox);
 int mdpd_batch_get_state(mdpd_batch_t *b, int32_t box, double *x, double *v, int64_t n);
 /* every box's x and v at once (x[k], v[k]: 3 n_k doubles each in tag order, as mdpd_batch_get_state
  * writes them; a null x[k] or v[k] skips that array; nbox must equal the batch's): all boxes'
- * tag gathers, then all copies back to back on the batch's stream and one wait, so the copies run
- * at the link's rate instead of one round trip per box.  Pinned host arrays make each copy a
- * direct DMA.  Device scratch of 6 sum(n_k) doubles for the call (from the box pool). */
+ * gathers and copies queued on the batch's stream with one wait at the end, instead of one host
+ * round trip per box.  Pinned host arrays make each copy a direct DMA.  Device scratch of 6 n_max
+ * doubles (the largest box) for the call, from the box pool. */
 int mdpd_batch_get_states(mdpd_batch_t *b, double *const *x, double *const *v, int32_t nbox);
 /* nsteps steps of every box, each step's thermo (every box, with that step's energy and virial:
  * a LAMMPS thermo line at every step, Run::command with thermo 1) written to

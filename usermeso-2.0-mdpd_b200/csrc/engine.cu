@@ -896,23 +896,20 @@ size_t Batch::thermo_bytes_per_step() const
 void Batch::download_all(double *const *x, double *const *v)
 {
     Range r("mdpd::download_all");
-    size_t total = 0;
-    for (const Box *b : boxes_) total += 6 * (size_t)b->n;
-    if (total == 0) return;
-    double *d = batch_alloc<double>(total, stream_);
-    size_t off = 0;
-    for (const Box *b : boxes_) {
-        launch_gather_by_tag(stream_, state_buffers(b->desc), b->desc.st, b->n, d + off, d + off + 3 * (size_t)b->n);
-        off += 6 * (size_t)b->n;
-    }
-    check_cuda(cudaGetLastError(), "download gather");
-    off = 0;
+    size_t nmax = 0;
+    for (const Box *b : boxes_) nmax = std::max(nmax, (size_t)b->n);
+    if (nmax == 0) return;
+    // one scratch of the largest box, reused box after box: the stream runs each box's gather
+    // after the previous box's copies have read the scratch, so nothing waits on the host
+    // until the end
+    double *d = batch_alloc<double>(6 * nmax, stream_);
     for (size_t k = 0; k < boxes_.size(); ++k) {
-        const size_t n3 = 3 * (size_t)boxes_[k]->n;
-        if (x[k]) check_cuda(cudaMemcpyAsync(x[k], d + off, sizeof(double) * n3, cudaMemcpyDeviceToHost, stream_), "download");
-        if (v[k])
-            check_cuda(cudaMemcpyAsync(v[k], d + off + n3, sizeof(double) * n3, cudaMemcpyDeviceToHost, stream_), "download");
-        off += 2 * n3;
+        const Box *b = boxes_[k];
+        const size_t n3 = 3 * (size_t)b->n;
+        launch_gather_by_tag(stream_, state_buffers(b->desc), b->desc.st, b->n, d, d + n3);
+        check_cuda(cudaGetLastError(), "download gather");
+        if (x[k]) check_cuda(cudaMemcpyAsync(x[k], d, sizeof(double) * n3, cudaMemcpyDeviceToHost, stream_), "download");
+        if (v[k]) check_cuda(cudaMemcpyAsync(v[k], d + n3, sizeof(double) * n3, cudaMemcpyDeviceToHost, stream_), "download");
     }
     check_cuda(cudaFreeAsync(d, stream_), "download scratch");
     check_cuda(cudaStreamSynchronize(stream_), "download");

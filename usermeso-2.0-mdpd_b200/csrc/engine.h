@@ -151,8 +151,8 @@ public:
     size_t thermo_bytes_per_step() const;  // device-to-host bytes run_thermo copies per step
     int status(std::string &msg);          // OR of box status words
     void read_states(std::vector<BoxState> &out);  // every box's device scalars, one copy
-    // every box's x, v in tag order into x[k], v[k] (null: skipped): the gathers, then the
-    // copies back to back on the batch's stream, one wait
+    // every box's x, v in tag order into x[k], v[k] (null: skipped): each box's gather and
+    // copies queued on the batch's stream through one scratch of the largest box, one wait
     void download_all(double *const *x, double *const *v);
     cudaStream_t stream() const { return stream_; }
     const std::vector<Box *> &boxes() const { return boxes_; }
