@@ -445,7 +445,7 @@ int mdpd_batch_create(mdpd_batch_t **out, const mdpd_box_spec *specs, int32_t nb
                 raw.push_back(b->boxes.back().get());
             }
         } catch (...) {
-            cudaStreamSynchronize(0);  // no queued copy reads the caller's arrays after the call
+            cudaDeviceSynchronize();  // no queued copy reads the caller's arrays after the call
             throw;
         }
         check_cuda(cudaStreamSynchronize(0), "upload");  // the caller's x, v are read by now

@@ -120,6 +120,22 @@ static cudaMemPool_t box_pool()
     return pools[dev];
 }
 
+// A box's arena is allocated, and the caller's x and v copied into it, on an upload stream of
+// the device (one per device, kept for the process); the legacy stream, which zeroes the arena
+// and runs the box's set-up kernels, waits for those copies. Boxes created one after another
+// then keep the copy engine busy: one box's copies overlap the previous box's kernels.
+static cudaStream_t upload_stream()
+{
+    static std::mutex mu;
+    static cudaStream_t streams[64] = {};
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "device");
+    if (dev < 0 || dev >= 64) throw std::runtime_error("CUDA device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!streams[dev]) check_cuda(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking), "upload stream");
+    return streams[dev];
+}
+
 size_t reserve_box_pool(size_t bytes)
 {
     // one allocation of the whole size, freed back at once: the pool keeps the memory mapped
@@ -369,9 +385,11 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
                                  std::to_string((long long)B.nrow * B.n_col) +
                                  " neighbour-table entries (limit 4294967295); split it into boxes");
     layout(s, na);  // size the arena
+    if (!x && !fill) throw std::runtime_error("ARG: no positions");
+    const cudaStream_t up = upload_stream();
     {
         void *a = nullptr;
-        const cudaError_t e = cudaMallocFromPoolAsync(&a, arena_need_, box_pool(), 0);
+        const cudaError_t e = cudaMallocFromPoolAsync(&a, arena_need_, box_pool(), up);
         if (e != cudaSuccess) {
             cudaGetLastError();
             throw std::runtime_error("OOM: device allocation of " + std::to_string(arena_need_) + " bytes failed");
@@ -379,6 +397,27 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
         arena_ = static_cast<char *>(a);
     }
     layout(s, na);  // hand out the pieces
+    // the caller's AoS x and v go to the list table's space (unused until the first build, which
+    // writes every entry it later reads) on the upload stream; the legacy stream waits for them
+    // before anything of its own touches the arena
+    const size_t stage_need = 6 * sizeof(double) * (size_t)n;
+    double *sx = reinterpret_cast<double *>(B.table), *sv = sx + 3 * (size_t)n;
+    {
+        if ((size_t)B.nrow * B.n_col * sizeof(int) < stage_need) {
+            cudaFreeAsync(arena_, up);
+            arena_ = nullptr;
+            throw std::runtime_error("ARG: list table too small to stage");
+        }
+        if (!fill) {
+            check_cuda(cudaMemcpyAsync(sx, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, up), "upload");
+            if (v) check_cuda(cudaMemcpyAsync(sv, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, up), "upload");
+        }
+        cudaEvent_t ev;
+        check_cuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "upload event");
+        check_cuda(cudaEventRecord(ev, up), "upload event");
+        check_cuda(cudaStreamWaitEvent(0, ev, 0), "upload event");
+        check_cuda(cudaEventDestroy(ev), "upload event");
+    }
     {
         // zero everything but the neighbour tables (most of the arena): every build writes each
         // list entry it later reads, and each density pass each compact entry
@@ -408,23 +447,14 @@ void Box::init(const Spec &s, const double *x, const double *v, const int32_t *t
 
     // Morton rank of every bin: reorder buckets are visited in Morton order of their bin
     launch_bin_ranks(0, g.mbin, B.bin_rank);
-    // initial state into buffer 0: the caller's AoS x and v (or a device fill of them) go to the
-    // list table's space (unused until the first build, which writes every entry it later
-    // reads), a kernel splits them into x, xh and v components and fills tags/types/masks that
-    // were not given
+    // initial state into buffer 0: the staged x and v (or a device fill of them), split by a
+    // kernel into x, xh and v components, which also fills tags/types/masks that were not given
     {
-        if (!x && !fill) throw std::runtime_error("ARG: no positions");
-        const size_t need = 6 * sizeof(double) * (size_t)n;
-        if ((size_t)B.nrow * B.n_col * sizeof(int) < need) throw std::runtime_error("ARG: list table too small to stage");
-        double *sx = reinterpret_cast<double *>(B.table), *sv = sx + 3 * (size_t)n;
         if (fill) {
             // the thermo partials (zeroed with the arena, rewritten by every thermo pass) hold
             // the fill's momentum sum
             launch_fill(0, *fill, s.lo, s.hi, n, sx, sv, reinterpret_cast<unsigned long long *>(B.partial));
             v = sv;  // non-null: the split kernel takes the filled velocities
-        } else {
-            check_cuda(cudaMemcpyAsync(sx, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, 0), "upload");
-            if (v) check_cuda(cudaMemcpyAsync(sv, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, 0), "upload");
         }
         if (tag) check_cuda(cudaMemcpyAsync(B.tag[0], tag, sizeof(int) * n, cudaMemcpyHostToDevice, 0), "upload");
         if (type) check_cuda(cudaMemcpyAsync(B.type[0], type, sizeof(int) * n, cudaMemcpyHostToDevice, 0), "upload");
